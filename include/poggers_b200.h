@@ -1,0 +1,164 @@
+/*
+ * poggers_b200.h -- C ABI of the poggers_b200 library (libpoggers_b200.so).
+ *
+ * B200-native (sm_100a) bulk operations on the POGGERS tables: the
+ * Two-Choice Filter (TCF) and the modular uint64 hash tables (double,
+ * linear and power-of-two probing over tile-cooperative buckets).
+ *
+ * Conventions (mirroring the reference where it has one):
+ *  - The library owns table memory; the caller owns every key, value and
+ *    result buffer.  Buffers passed as d_* are device pointers.
+ *  - Every bulk call is asynchronous and ordered on the given stream
+ *    (NULL = the legacy default stream).  Calls on the same table must be
+ *    phase-separated by stream order: the reference's guarantee that a query
+ *    sees an insert holds only across kernel boundaries, and so does ours.
+ *  - Errors are status codes, never exceptions or device traps.  The
+ *    reference throws std::runtime_error on a sizing mismatch
+ *    (tables/base_table.cuh:116-131) and returns bool from device ops.
+ *  - Counters passed as d_count are ADDED to (like the reference test
+ *    harness's atomicAdd on a caller-zeroed counter); zero them first.
+ *  - Values are typed by the table format: uint64_t for PG_FMT_KV64,
+ *    uint16_t for PG_FMT_TAGVAL16; PG_FMT_TAG16 stores no values and reports
+ *    0, like key_container::get_val (representations/key_only.cuh:75-77).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   pg_table_create   <- static_table::generate_on_device(Sizing*, seed)      tables/base_table.cuh:110-145
+ *   pg_table_destroy  <- static_table::free_on_device(Table*)                tables/base_table.cuh:147-164
+ *   pg_bulk_insert    <- insert(tile, key, val) launched one tile per key     tables/base_table.cuh:167-187,
+ *                        with get_num_blocks / get_block_size                 tables/base_table.cuh:321-329
+ *                        (bulk driver shape: tests/src/test_mhm_tcf.cu:319-345)
+ *   pg_bulk_query     <- query(tile, key, Val&)                               tables/base_table.cuh:273-290
+ *                        (driver: tests/src/test_mhm_tcf.cu:457-521)
+ *   pg_bulk_remove    <- remove(tile, key)                                    tables/base_table.cuh:292-308
+ *                        (driver: tests/src/delete_tests.cu:336-372)
+ *   pg_table_count_fill <- count_fill_kernel / get_fill                       tables/bucketed_table.cuh:37-52,498-548
+ *   pg_table_bytes    <- host_bytes_in_use                                    tables/base_table.cuh:331-351
+ */
+#ifndef POGGERS_B200_H
+#define POGGERS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ABI-compatible with cudaStream_t, without requiring the CUDA headers. */
+typedef struct CUstream_st *pg_stream_t;
+
+typedef enum pg_status {
+    PG_OK = 0,
+    PG_ERR_INVALID = 1,     /* bad argument or configuration */
+    PG_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    PG_ERR_NOMEM = 3,       /* device allocation failed */
+    PG_ERR_UNSUPPORTED = 4, /* valid but not compiled in (bucket size / tile combination) */
+    PG_ERR_FULL = 5,        /* capacity exhausted */
+    PG_ERR_TIMEOUT = 6      /* a bounded device wait gave up */
+} pg_status;
+
+/* slot formats (reference representations) */
+enum {
+    PG_FMT_KV64 = 0,     /* key_val_pair<uint64_t,uint64_t>: the modular hash tables */
+    PG_FMT_TAGVAL16 = 1, /* dynamic_container<key_val_pair,uint16_t>: the TCF (16-bit tag + 16-bit val) */
+    PG_FMT_TAG16 = 2     /* dynamic_container<key_container,uint16_t>: tag-only TCF */
+};
+
+/* insert schemes */
+enum {
+    PG_SCHEME_BUCKET = 0,     /* insert_schemes/bucket_insert.cuh */
+    PG_SCHEME_TWO_CHOICE = 1  /* insert_schemes/power_of_n_shortcut.cuh (max_probes <= 8) */
+};
+
+/* probing schemes */
+enum {
+    PG_PROBE_DOUBLE = 0,  /* probing_schemes/double_hashing.cuh */
+    PG_PROBE_LINEAR = 1,  /* probing_schemes/linear_probing.cuh */
+    PG_PROBE_P2 = 2,      /* probing_schemes/power_of_two.cuh (max_probes == 2) */
+    PG_PROBE_XOR_P2 = 3   /* probing_schemes/xor_power_of_two.cuh (max_probes == 2) */
+};
+
+typedef struct pg_level_config {
+    uint64_t nslots;      /* requested slots; buckets = ceil(nslots / bucket_size) */
+    uint32_t bucket_size; /* level 0: 4, 8, 16 or 32; level 1: 1..64 */
+    uint32_t max_probes;
+    uint32_t scheme;      /* PG_SCHEME_* */
+    uint32_t probe;       /* PG_PROBE_* */
+} pg_level_config;
+
+typedef struct pg_table_config {
+    uint32_t format;   /* PG_FMT_* */
+    uint32_t tile;     /* lanes per key (the reference's Partition_Size): 1,2,4,8,16; <= level-0 bucket size */
+    uint32_t nlevels;  /* 1, or 2 = primary + backing (static_table's recursive table) */
+    uint32_t reserved; /* must be 0 */
+    pg_level_config levels[2];
+} pg_table_config;
+
+typedef struct pg_level_info {
+    uint64_t nbuckets;
+    uint64_t nslots;       /* nbuckets * bucket_size */
+    uint64_t bytes;        /* device bytes of the bucket array */
+    uint64_t seed;         /* level seed (level 0: the table seed, level 1: seed*seed) */
+    const void *d_buckets; /* device address of the bucket array */
+} pg_level_info;
+
+typedef struct pg_table pg_table;
+
+/* Library version string, e.g. "poggers_b200 0.1 sm_100a". */
+const char *pg_version(void);
+const char *pg_status_string(pg_status s);
+
+/* Create a table on the current device; slot arrays are zeroed.  Level l is
+ * hashed with seed^(2^l) exactly like static_table::generate_on_device. */
+pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **out);
+pg_status pg_table_destroy(pg_table *t);
+/* Zero every slot (stream-ordered). */
+pg_status pg_table_clear(pg_table *t, pg_stream_t stream);
+pg_status pg_table_level_info(const pg_table *t, uint32_t level, pg_level_info *out);
+/* Device bytes owned by the table (host_bytes_in_use). */
+uint64_t pg_table_bytes(const pg_table *t);
+
+/* Launch shape: threads per block (multiple of the tile, <= 1024) and a cap on
+ * blocks (0 = enough blocks for one key per group, capped at blocks_per_sm
+ * resident blocks on every SM).  block_threads == tile with max_blocks == 1
+ * runs the batch strictly in order on one group (deterministic layout). */
+pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks);
+
+/* Bulk insert of n keys (and values; d_vals may be NULL = all 0).
+ * d_ok[i] (optional) = 1 if key i was placed; d_fail_count (optional) += failures. */
+pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                         uint8_t *d_ok, uint64_t *d_fail_count, pg_stream_t stream);
+
+/* Bulk query: d_vals_out[i] (optional) = value found (0 if absent);
+ * d_found[i] (optional) = 1 if present; d_hit_count (optional) += hits. */
+pg_status pg_bulk_query(pg_table *t, const uint64_t *d_keys, uint64_t n, void *d_vals_out,
+                        uint8_t *d_found, uint64_t *d_hit_count, pg_stream_t stream);
+
+/* Bulk remove (tombstones): d_ok[i] (optional) = 1 if a matching slot was
+ * removed; d_hit_count (optional) += removals. */
+pg_status pg_bulk_remove(pg_table *t, const uint64_t *d_keys, uint64_t n, uint8_t *d_ok,
+                         uint64_t *d_hit_count, pg_stream_t stream);
+
+/* d_out[0] += occupied (non-empty) slots of `level`, d_out[1] += tombstones. */
+pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_stream_t stream);
+
+/* Copy a level to / from host memory in the REFERENCE's slot layout
+ * (array of {key, val} structs, buckets of bucket_size consecutive slots),
+ * so dumps compare byte-for-byte with the reference's device table and can
+ * be reloaded.  `bytes` must equal nslots * slot size (16, 4 or 2 bytes).
+ * Synchronous. */
+pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst, uint64_t bytes);
+pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes);
+
+/* Host-side helpers used by tests (no GPU needed). */
+uint64_t pg_host_murmur64a(uint64_t key, uint64_t seed);
+uint64_t pg_host_fastmod(uint64_t n, uint64_t d);
+/* Bucket ids (after % nbuckets) a table level probes for `key`; returns count. */
+uint32_t pg_host_probe_buckets(const pg_table_config *cfg, uint32_t level, uint64_t seed, uint64_t key,
+                               uint64_t *out, uint32_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POGGERS_B200_H */

@@ -1,0 +1,702 @@
+// level.cuh -- device-side bucket operations of one table level.
+//
+// A level is one insert scheme over its own bucket array: bucket_insert
+// (include/poggers/insert_schemes/bucket_insert.cuh) or the two-choice
+// shortcut scheme (include/poggers/insert_schemes/power_of_n_shortcut.cuh).
+// A table is one level, or a primary level backed by a second one, exactly
+// like the reference's static_table with a recursive backing table
+// (include/poggers/tables/base_table.cuh:167-308).
+//
+// Layout in HBM (B = bucket size):
+//   bucket b = [ B keys | B vals ], b * B * (sizeof K + sizeof V) bytes in.
+// Keys of a bucket are contiguous, so a group of G lanes reads them with one
+// 16-byte (or narrower) load per lane and the vals are touched only at the
+// one slot a query returns or an insert writes.  The reference keeps the
+// same slots as {key, val} structs; converting between the two layouts is a
+// pure permutation (see pg_table_dump_level).
+//
+// One key is served by a group of G consecutive lanes (the reference's
+// tile, `cg::thread_block_tile<Partition_Size>`), built on
+// __ballot_sync / __shfl_sync / __reduce_add_sync with the group's own lane
+// mask instead of cooperative-groups partitions.
+//
+// Semantics kept from the reference (sentinels included):
+//   empty key 0, tombstone = empty - 1 (key_val_pair.cuh:70,115-117);
+//   insert = CAS(empty -> key) on the first empty slot of a probed bucket in
+//            slot order, then a plain val store (key_val_pair.cuh:84-95);
+//   remove = CAS(key -> tombstone) on the first matching slot, val untouched;
+//   bucket_insert query / remove stop at the first bucket holding an empty
+//            slot (bucket_insert.cuh:283-285, 338-345);
+//   two-choice query / remove visit every probed bucket, two-choice insert
+//            takes a bucket whose fill is below 3/4 at once and otherwise the
+//            least-filled bucket first (power_of_n_shortcut.cuh:327-435).
+// Filled slots always form a prefix of each bucket (an insert only takes an
+// empty slot after every earlier slot of its snapshot was seen filled, and
+// nothing turns a filled slot back to empty), so the reference's per-stripe
+// early exit equals "first match at or before the first empty slot", which
+// is what is computed here for any group width G.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+#include "hash.cuh"
+
+namespace pg {
+
+enum fmt_kind : uint32_t { FMT_KV64 = 0, FMT_TAGVAL16 = 1, FMT_TAG16 = 2 };
+enum scheme_kind : uint32_t { SCHEME_BUCKET = 0, SCHEME_TWO_CHOICE = 1 };
+
+constexpr int kTwoChoiceMaxProbes = 4;
+
+struct level_desc {
+    unsigned char *base;   // bucket array
+    fastmod64 nbmod;       // d = number of buckets
+    uint64_t seed, seed2;  // hasher seeds (s, s*s)
+    uint32_t bucket_size, max_probes, scheme, probe;
+    uint32_t bucket_bytes, val_offset;
+};
+
+struct table_desc {
+    level_desc lv[2];
+    uint32_t nlevels, format;
+};
+
+template <int FMT> struct fmt_t;
+template <> struct fmt_t<FMT_KV64> {
+    using K = unsigned long long;
+    using V = unsigned long long;
+    static constexpr bool kHasVal = true;
+    static constexpr K kTomb = ~0ULL;
+    PG_HD static K stored(uint64_t key) { return key; }
+    PG_HD static uint64_t tag(uint64_t key) { return key; }
+};
+template <> struct fmt_t<FMT_TAGVAL16> {
+    using K = unsigned short;
+    using V = unsigned short;
+    static constexpr bool kHasVal = true;
+    static constexpr K kTomb = 0xFFFFu;
+    PG_HD static K stored(uint64_t key) { return tag16(key); }
+    PG_HD static uint64_t tag(uint64_t key) { return tag16(key); }
+};
+template <> struct fmt_t<FMT_TAG16> {
+    using K = unsigned short;
+    using V = unsigned short;  // key_container: queries report val 0
+    static constexpr bool kHasVal = false;
+    static constexpr K kTomb = 0xFFFFu;
+    PG_HD static K stored(uint64_t key) { return tag16(key); }
+    PG_HD static uint64_t tag(uint64_t key) { return tag16(key); }
+};
+
+// ---------------------------------------------------------------- groups
+template <int G>
+struct group {
+    uint32_t gl;     // lane inside the group
+    uint32_t gbase;  // warp lane of the group's lane 0
+    uint32_t gmask;  // the group's lanes in the warp
+
+    __device__ __forceinline__ static group make()
+    {
+        group g;
+        uint32_t lane = threadIdx.x & 31u;
+        g.gl = lane & (G - 1);
+        g.gbase = lane - g.gl;
+        g.gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << g.gbase);
+        return g;
+    }
+    __device__ __forceinline__ uint32_t ballot(bool p) const
+    {
+        uint32_t b = __ballot_sync(gmask, p);
+        return (G == 32) ? b : ((b >> gbase) & ((1u << G) - 1u));
+    }
+    template <class T>
+    __device__ __forceinline__ T shfl(T v, uint32_t src_gl) const
+    {
+        if constexpr (sizeof(T) < 4) return (T)__shfl_sync(gmask, (unsigned)v, gbase + src_gl);
+        else return __shfl_sync(gmask, v, gbase + src_gl);
+    }
+    __device__ __forceinline__ uint32_t sum(uint32_t v) const { return __reduce_add_sync(gmask, v); }
+};
+
+// ---------------------------------------------------------------- loads
+// L2-only loads (ld.global.cg): buckets are touched once per key, and a
+// bucket another SM just updated by CAS must not be served from a stale L1.
+template <class K, int N>
+__device__ __forceinline__ void load_keys(const K *p, K (&k)[N])
+{
+    constexpr int BYTES = N * (int)sizeof(K);
+    if constexpr (BYTES >= 16) {
+        static_assert(BYTES % 16 == 0, "vector width");
+#pragma unroll
+        for (int v = 0; v < BYTES / 16; ++v) {
+            uint4 x = __ldcg(reinterpret_cast<const uint4 *>(p) + v);
+            memcpy(reinterpret_cast<char *>(k) + 16 * v, &x, 16);
+        }
+    } else if constexpr (BYTES == 8) {
+        uint2 x = __ldcg(reinterpret_cast<const uint2 *>(p));
+        memcpy(k, &x, 8);
+    } else if constexpr (BYTES == 4) {
+        unsigned int x = __ldcg(reinterpret_cast<const unsigned int *>(p));
+        memcpy(k, &x, 4);
+    } else {
+        static_assert(BYTES == 2, "vector width");
+        unsigned short x = __ldcg(reinterpret_cast<const unsigned short *>(p));
+        memcpy(k, &x, 2);
+    }
+}
+
+template <class K, int N>
+__device__ __forceinline__ uint32_t eq_mask(const K (&k)[N], K v)
+{
+    uint32_t m = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) m |= (uint32_t)(k[i] == v) << i;
+    return m;
+}
+
+template <class T>
+__device__ __forceinline__ T ldcg_scalar(const T *p)
+{
+    return __ldcg(p);
+}
+
+// ---------------------------------------------------------------- level ops
+// Compile-time bucket size B served by groups of G lanes.  Lane gl < ACT
+// owns slots [gl*N, gl*N + N).
+template <int FMT, int B, int G>
+struct level_ops {
+    using F = fmt_t<FMT>;
+    using K = typename F::K;
+    using V = typename F::V;
+    static constexpr int ACT = B < G ? B : G;
+    static constexpr int N = B < G ? 1 : B / G;
+    static_assert(N <= 32, "slots per lane");
+
+    __device__ __forceinline__ static K *keys_of(const level_desc &L, uint64_t b)
+    {
+        return reinterpret_cast<K *>(L.base + b * (uint64_t)L.bucket_bytes);
+    }
+    __device__ __forceinline__ static V *vals_of(const level_desc &L, uint64_t b)
+    {
+        return reinterpret_cast<V *>(L.base + b * (uint64_t)L.bucket_bytes + L.val_offset);
+    }
+
+    // This lane's keys of bucket b; lanes past the bucket hold no slot.
+    __device__ __forceinline__ static void load(const level_desc &L, const group<G> &g, uint64_t b, K (&k)[N],
+                                                bool &active)
+    {
+        active = (int)g.gl < ACT;
+        if (active) load_keys<K, N>(keys_of(L, b) + g.gl * N, k);
+        else {
+#pragma unroll
+            for (int i = 0; i < N; ++i) k[i] = F::kTomb;  // neither empty nor a stored key's slot
+        }
+    }
+
+    // first slot (in slot order) whose lane-local bit is set, or -1
+    __device__ __forceinline__ static int first(const group<G> &g, uint32_t m)
+    {
+        uint32_t bal = g.ballot(m != 0);
+        if (!bal) return -1;
+        uint32_t ln = __ffs(bal) - 1;
+        int bit = g.shfl((int)__ffs(m) - 1, ln);
+        return (int)ln * N + bit;
+    }
+
+    // CAS(empty -> sk) on the empty slots of the snapshot, in slot order.
+    __device__ __forceinline__ static bool insert_into(const level_desc &L, const group<G> &g, uint64_t b, K sk,
+                                                       V val, uint32_t emp)
+    {
+        while (true) {
+            uint32_t bal = g.ballot(emp != 0);
+            if (!bal) return false;
+            uint32_t leader = __ffs(bal) - 1;
+            bool ok = false;
+            if (g.gl == leader) {
+                int i = __ffs(emp) - 1;
+                int slot = (int)g.gl * N + i;
+                if (atomicCAS(keys_of(L, b) + slot, (K)0, sk) == (K)0) {
+                    ok = true;
+                    if constexpr (F::kHasVal) vals_of(L, b)[slot] = val;
+                } else {
+                    emp &= emp - 1;
+                }
+            }
+            if (g.ballot(ok)) return true;
+        }
+    }
+
+    // CAS(sk -> tombstone) on the matching slots, in slot order.
+    __device__ __forceinline__ static bool remove_from(const level_desc &L, const group<G> &g, uint64_t b, K sk,
+                                                       uint32_t match)
+    {
+        while (true) {
+            uint32_t bal = g.ballot(match != 0);
+            if (!bal) return false;
+            uint32_t leader = __ffs(bal) - 1;
+            bool ok = false;
+            if (g.gl == leader) {
+                int i = __ffs(match) - 1;
+                int slot = (int)g.gl * N + i;
+                if (atomicCAS(keys_of(L, b) + slot, sk, F::kTomb) == sk) ok = true;
+                else match &= match - 1;
+            }
+            if (g.ballot(ok)) return true;
+        }
+    }
+
+    __device__ __forceinline__ static V read_val(const level_desc &L, const group<G> &g, uint64_t b, int slot)
+    {
+        if constexpr (!F::kHasVal) {
+            return (V)0;
+        } else {
+            V v = 0;
+            if ((int)g.gl == slot / N) v = ldcg_scalar(vals_of(L, b) + slot);
+            return g.shfl(v, (uint32_t)(slot / N));
+        }
+    }
+
+    __device__ __forceinline__ static void begin(const level_desc &L, uint64_t key, probe_seq &ps)
+    {
+        ps.begin(L.probe, key, F::tag(key), L.seed, L.seed2);
+    }
+
+    // ---- insert: bucket_insert (bucket_insert.cuh:127-203)
+    __device__ static bool insert_bucket_scheme(const level_desc &L, const group<G> &g, uint64_t key, V val)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        begin(L, key, ps);
+        for (uint32_t i = 0; i < L.max_probes; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            K k[N];
+            bool act;
+            load(L, g, b, k, act);
+            uint32_t emp = act ? eq_mask(k, (K)0) : 0u;
+            if (insert_into(L, g, b, sk, val, emp)) return true;
+        }
+        return false;
+    }
+
+    // ---- insert: two-choice shortcut (power_of_n_shortcut.cuh:327-435).
+    // Probe bookkeeping is unrolled over kTwoChoiceMaxProbes so it stays in
+    // registers; both choices of the common 2-probe case are fetched together.
+    __device__ static bool insert_two_choice(const level_desc &L, const group<G> &g, uint64_t key, V val)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        begin(L, key, ps);
+        constexpr int MP = kTwoChoiceMaxProbes;
+        uint64_t bk[MP];
+        int fill[MP];
+        int np = 0, min_fill = B;
+        K k1[N];
+        bool act1 = false, have1 = false;
+        if (L.max_probes >= 2 && ps.at(0) != kProbeEnd && ps.at(1) != kProbeEnd) {
+            load(L, g, L.nbmod.mod(ps.at(1)), k1, act1);
+            have1 = true;
+        }
+        bool stop = false;
+#pragma unroll
+        for (int i = 0; i < MP; ++i) {
+            bk[i] = 0;
+            fill[i] = B;
+            if (stop || (uint32_t)i >= L.max_probes) continue;
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) {
+                stop = true;
+                continue;
+            }
+            uint64_t b = L.nbmod.mod(raw);
+            K k[N];
+            bool act;
+            if (i == 1 && have1) {
+#pragma unroll
+                for (int j = 0; j < N; ++j) k[j] = k1[j];
+                act = act1;
+            } else {
+                load(L, g, b, k, act);
+            }
+            uint32_t emp = act ? eq_mask(k, (K)0) : 0u;
+            int f = (int)g.sum(act ? (uint32_t)(N - __popc(emp)) : 0u);
+            bk[i] = b;
+            if (4 * f < 3 * B) {
+                if (insert_into(L, g, b, sk, val, emp)) return true;
+                f = B;
+            }
+            fill[i] = f;
+            if (f < min_fill) min_fill = f;
+            np = i + 1;
+        }
+        int lvl = min_fill;
+        while (lvl < B) {
+            int next = B;
+#pragma unroll
+            for (int j = 0; j < MP; ++j) {
+                if (j < np && fill[j] == lvl) {
+                    K k[N];
+                    bool act;
+                    load(L, g, bk[j], k, act);
+                    uint32_t emp = act ? eq_mask(k, (K)0) : 0u;
+                    if (insert_into(L, g, bk[j], sk, val, emp)) return true;
+                }
+                if (j < np && fill[j] > lvl && fill[j] < next) next = fill[j];
+            }
+            lvl = next;
+        }
+        return false;
+    }
+
+    template <int SCHEME>
+    __device__ __forceinline__ static bool insert_s(const level_desc &L, const group<G> &g, uint64_t key, V val)
+    {
+        if constexpr (SCHEME == SCHEME_BUCKET) return insert_bucket_scheme(L, g, key, val);
+        else return insert_two_choice(L, g, key, val);
+    }
+    __device__ __forceinline__ static bool insert(const level_desc &L, const group<G> &g, uint64_t key, V val)
+    {
+        return L.scheme == SCHEME_BUCKET ? insert_bucket_scheme(L, g, key, val) : insert_two_choice(L, g, key, val);
+    }
+
+    // ---- query: bucket_insert (bucket_insert.cuh:295-357)
+    __device__ static bool query_bucket_scheme(const level_desc &L, const group<G> &g, uint64_t key, V &out)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        begin(L, key, ps);
+        {
+            for (uint32_t i = 0; i < L.max_probes; ++i) {
+                uint64_t raw = ps.at(i);
+                if (raw == kProbeEnd) break;
+                uint64_t b = L.nbmod.mod(raw);
+                K k[N];
+                bool act;
+                load(L, g, b, k, act);
+                int fm = first(g, act ? eq_mask(k, sk) : 0u);
+                int fe = first(g, act ? eq_mask(k, (K)0) : 0u);
+                if (fm >= 0 && (fe < 0 || fm <= fe)) {
+                    out = read_val(L, g, b, fm);
+                    return true;
+                }
+                if (fe >= 0) return false;
+            }
+            return false;
+        }
+    }
+
+    // ---- query: two-choice (power_of_n_shortcut.cuh:193-232, 437-468): every
+    // probed bucket, no early exit; the first two are fetched together
+    __device__ static bool query_two_choice(const level_desc &L, const group<G> &g, uint64_t key, V &out)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        begin(L, key, ps);
+        uint64_t r0 = ps.at(0);
+        if (r0 == kProbeEnd) return false;
+        uint64_t b0 = L.nbmod.mod(r0);
+        K k0[N], k1[N];
+        bool a0, a1 = false;
+        uint64_t b1 = 0;
+        bool two = L.max_probes >= 2 && ps.at(1) != kProbeEnd;
+        load(L, g, b0, k0, a0);
+        if (two) {
+            b1 = L.nbmod.mod(ps.at(1));
+            load(L, g, b1, k1, a1);
+        }
+        int fm = first(g, a0 ? eq_mask(k0, sk) : 0u);
+        if (fm >= 0) {
+            out = read_val(L, g, b0, fm);
+            return true;
+        }
+        if (!two) return false;
+        fm = first(g, a1 ? eq_mask(k1, sk) : 0u);
+        if (fm >= 0) {
+            out = read_val(L, g, b1, fm);
+            return true;
+        }
+        for (uint32_t i = 2; i < L.max_probes; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            K k[N];
+            bool act;
+            load(L, g, b, k, act);
+            fm = first(g, act ? eq_mask(k, sk) : 0u);
+            if (fm >= 0) {
+                out = read_val(L, g, b, fm);
+                return true;
+            }
+        }
+        return false;
+    }
+
+    template <int SCHEME>
+    __device__ __forceinline__ static bool query_s(const level_desc &L, const group<G> &g, uint64_t key, V &out)
+    {
+        if constexpr (SCHEME == SCHEME_BUCKET) return query_bucket_scheme(L, g, key, out);
+        else return query_two_choice(L, g, key, out);
+    }
+    __device__ __forceinline__ static bool query(const level_desc &L, const group<G> &g, uint64_t key, V &out)
+    {
+        return L.scheme == SCHEME_BUCKET ? query_bucket_scheme(L, g, key, out) : query_two_choice(L, g, key, out);
+    }
+
+    // ---- remove: bucket_insert stops at a bucket holding an empty slot
+    // (bucket_insert.cuh:205-293); two-choice visits every probe
+    // (power_of_n_shortcut.cuh:263-325, 470-501)
+    template <int SCHEME>
+    __device__ static bool remove_s(const level_desc &L, const group<G> &g, uint64_t key)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        begin(L, key, ps);
+        constexpr bool early = (SCHEME == SCHEME_BUCKET);
+        for (uint32_t i = 0; i < L.max_probes; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            K k[N];
+            bool act;
+            load(L, g, b, k, act);
+            uint32_t match = act ? eq_mask(k, sk) : 0u;
+            uint32_t emp = act ? (eq_mask(k, (K)0) & ~match) : 0u;
+            if (remove_from(L, g, b, sk, match)) return true;
+            if (early && g.ballot(emp != 0)) return false;
+        }
+        return false;
+    }
+    __device__ __forceinline__ static bool remove(const level_desc &L, const group<G> &g, uint64_t key)
+    {
+        return L.scheme == SCHEME_BUCKET ? remove_s<SCHEME_BUCKET>(L, g, key) : remove_s<SCHEME_TWO_CHOICE>(L, g, key);
+    }
+};
+
+// Runtime bucket size (any B >= 1): the reference's own stripe walk, lane gl
+// owns slots gl, gl+G, gl+2G, ...  Serves backing levels whose bucket size
+// differs from the primary's.
+template <int FMT, int G>
+struct level_ops_dyn {
+    using F = fmt_t<FMT>;
+    using K = typename F::K;
+    using V = typename F::V;
+
+    __device__ __forceinline__ static K *keys_of(const level_desc &L, uint64_t b)
+    {
+        return reinterpret_cast<K *>(L.base + b * (uint64_t)L.bucket_bytes);
+    }
+    __device__ __forceinline__ static V *vals_of(const level_desc &L, uint64_t b)
+    {
+        return reinterpret_cast<V *>(L.base + b * (uint64_t)L.bucket_bytes + L.val_offset);
+    }
+    __device__ __forceinline__ static K key_at(const level_desc &L, uint64_t b, uint32_t s)
+    {
+        return ldcg_scalar(keys_of(L, b) + s);
+    }
+
+    // first slot index in slot order satisfying pred, or -1
+    template <class P>
+    __device__ __forceinline__ static int first(const level_desc &L, const group<G> &g, uint64_t b, P pred)
+    {
+        const uint32_t B = L.bucket_size;
+        for (uint32_t s0 = 0; s0 < B; s0 += G) {
+            uint32_t s = s0 + g.gl;
+            bool p = s < B && pred(key_at(L, b, s));
+            uint32_t bal = g.ballot(p);
+            if (bal) return (int)(s0 + __ffs(bal) - 1);
+        }
+        return -1;
+    }
+
+    __device__ static bool insert_bucket(const level_desc &L, const group<G> &g, uint64_t b, K sk, V val)
+    {
+        const uint32_t B = L.bucket_size;
+        for (uint32_t s0 = 0; s0 < B; s0 += G) {
+            uint32_t s = s0 + g.gl;
+            bool e = s < B && key_at(L, b, s) == (K)0;
+            uint32_t bal = g.ballot(e);
+            while (bal) {
+                uint32_t leader = __ffs(bal) - 1;
+                bool ok = false;
+                if (g.gl == leader && atomicCAS(keys_of(L, b) + s, (K)0, sk) == (K)0) {
+                    ok = true;
+                    if constexpr (F::kHasVal) vals_of(L, b)[s] = val;
+                }
+                if (g.ballot(ok)) return true;
+                bal &= bal - 1;
+            }
+        }
+        return false;
+    }
+
+    __device__ static bool remove_bucket(const level_desc &L, const group<G> &g, uint64_t b, K sk)
+    {
+        const uint32_t B = L.bucket_size;
+        for (uint32_t s0 = 0; s0 < B; s0 += G) {
+            uint32_t s = s0 + g.gl;
+            bool m = s < B && key_at(L, b, s) == sk;
+            uint32_t bal = g.ballot(m);
+            while (bal) {
+                uint32_t leader = __ffs(bal) - 1;
+                bool ok = false;
+                if (g.gl == leader && atomicCAS(keys_of(L, b) + s, sk, F::kTomb) == sk) ok = true;
+                if (g.ballot(ok)) return true;
+                bal &= bal - 1;
+            }
+        }
+        return false;
+    }
+
+    __device__ static V read_val(const level_desc &L, uint64_t b, int slot)
+    {
+        if constexpr (!F::kHasVal) return (V)0;
+        else return ldcg_scalar(vals_of(L, b) + slot);
+    }
+
+    __device__ static int fill_of(const level_desc &L, const group<G> &g, uint64_t b)
+    {
+        const uint32_t B = L.bucket_size;
+        uint32_t c = 0;
+        for (uint32_t s = g.gl; s < B; s += G) c += key_at(L, b, s) != (K)0;
+        return (int)g.sum(c);
+    }
+
+    __device__ static bool insert(const level_desc &L, const group<G> &g, uint64_t key, V val)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        ps.begin(L.probe, key, F::tag(key), L.seed, L.seed2);
+        if (L.scheme == SCHEME_BUCKET) {
+            for (uint32_t i = 0; i < L.max_probes; ++i) {
+                uint64_t raw = ps.at(i);
+                if (raw == kProbeEnd) break;
+                if (insert_bucket(L, g, L.nbmod.mod(raw), sk, val)) return true;
+            }
+            return false;
+        }
+        const int B = (int)L.bucket_size;
+        uint64_t bk[kTwoChoiceMaxProbes];
+        int fill[kTwoChoiceMaxProbes];
+        int np = 0, min_fill = B;
+        const uint32_t mp = L.max_probes < (uint32_t)kTwoChoiceMaxProbes ? L.max_probes : kTwoChoiceMaxProbes;
+        for (uint32_t i = 0; i < mp; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            int f = fill_of(L, g, b);
+            bk[np] = b;
+            if (4 * f < 3 * B) {
+                if (insert_bucket(L, g, b, sk, val)) return true;
+                f = B;
+            }
+            fill[np] = f;
+            if (f < min_fill) min_fill = f;
+            ++np;
+        }
+        int lvl = min_fill;
+        while (lvl < B) {
+            int next = B;
+            for (int j = 0; j < np; ++j) {
+                if (fill[j] == lvl && insert_bucket(L, g, bk[j], sk, val)) return true;
+                if (fill[j] > lvl && fill[j] < next) next = fill[j];
+            }
+            lvl = next;
+        }
+        return false;
+    }
+
+    __device__ static bool query(const level_desc &L, const group<G> &g, uint64_t key, V &out)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        ps.begin(L.probe, key, F::tag(key), L.seed, L.seed2);
+        const bool early = (L.scheme == SCHEME_BUCKET);
+        for (uint32_t i = 0; i < L.max_probes; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            int fm = first(L, g, b, [sk](K k) { return k == sk; });
+            int fe = early ? first(L, g, b, [](K k) { return k == (K)0; }) : -1;
+            if (fm >= 0 && (fe < 0 || fm <= fe)) {
+                out = read_val(L, b, fm);
+                return true;
+            }
+            if (fe >= 0) return false;
+        }
+        return false;
+    }
+
+    __device__ static bool remove(const level_desc &L, const group<G> &g, uint64_t key)
+    {
+        const K sk = F::stored(key);
+        probe_seq ps;
+        ps.begin(L.probe, key, F::tag(key), L.seed, L.seed2);
+        const bool early = (L.scheme == SCHEME_BUCKET);
+        for (uint32_t i = 0; i < L.max_probes; ++i) {
+            uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) break;
+            uint64_t b = L.nbmod.mod(raw);
+            if (remove_bucket(L, g, b, sk)) return true;
+            if (early && first(L, g, b, [sk](K k) { return k == (K)0 && k != sk; }) >= 0) return false;
+        }
+        return false;
+    }
+};
+
+// ---------------------------------------------------------------- table ops
+// static_table dispatch: the primary level (compile-time bucket size B0 and
+// scheme S0), then the backing level on failure or miss
+// (base_table.cuh:167-187, 273-308).  The backing level is entered out of
+// line so its registers do not weigh on the primary path.
+template <int FMT, int G>
+struct backing_ops {
+    using F = fmt_t<FMT>;
+    using V = typename F::V;
+    using L1 = level_ops_dyn<FMT, G>;
+    using L1x4 = level_ops<FMT, 4, G>;
+    __device__ __noinline__ static bool insert(const level_desc L, const group<G> g, uint64_t key, V val)
+    {
+        if (L.bucket_size == 4 && G <= 4) return L1x4::insert(L, g, key, val);
+        return L1::insert(L, g, key, val);
+    }
+    __device__ __noinline__ static bool query(const level_desc L, const group<G> g, uint64_t key, V *val)
+    {
+        V v = 0;
+        bool r = (L.bucket_size == 4 && G <= 4) ? L1x4::query(L, g, key, v) : L1::query(L, g, key, v);
+        *val = v;
+        return r;
+    }
+    __device__ __noinline__ static bool remove(const level_desc L, const group<G> g, uint64_t key)
+    {
+        if (L.bucket_size == 4 && G <= 4) return L1x4::remove(L, g, key);
+        return L1::remove(L, g, key);
+    }
+};
+
+template <int FMT, int B0, int G, int S0, bool BK_ON = true>
+struct table_ops {
+    using F = fmt_t<FMT>;
+    using V = typename F::V;
+    using L0 = level_ops<FMT, B0, G>;
+    using BK = backing_ops<FMT, G>;
+
+    __device__ __forceinline__ static bool insert(const table_desc &t, const group<G> &g, uint64_t key, V val)
+    {
+        if (L0::template insert_s<S0>(t.lv[0], g, key, val)) return true;
+        if (!BK_ON || t.nlevels < 2) return false;
+        return BK::insert(t.lv[1], g, key, val);
+    }
+    __device__ __forceinline__ static bool query(const table_desc &t, const group<G> &g, uint64_t key, V &val)
+    {
+        if (L0::template query_s<S0>(t.lv[0], g, key, val)) return true;
+        if (!BK_ON || t.nlevels < 2) return false;
+        return BK::query(t.lv[1], g, key, &val);
+    }
+    __device__ __forceinline__ static bool remove(const table_desc &t, const group<G> &g, uint64_t key)
+    {
+        if (L0::template remove_s<S0>(t.lv[0], g, key)) return true;
+        if (!BK_ON || t.nlevels < 2) return false;
+        return BK::remove(t.lv[1], g, key);
+    }
+};
+
+}  // namespace pg

@@ -1,0 +1,207 @@
+"""ctypes loader for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this.
+It wraps oracle/_build/libpoggers_oracle.so (the C restatement of the
+reference's table algorithms) and, when present, oracle/_ref/*.so (the
+reference's own code compiled from its sources by oracle/Makefile).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libpoggers_oracle.so"
+REFHOST_PATH = HERE / "_ref" / "libpoggers_refhost.so"
+REFCUDA_PATH = HERE / "_ref" / "libpoggers_refcuda.so"
+
+FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
+SCHEME_BUCKET, SCHEME_TWO_CHOICE = 0, 1
+PROBE_DOUBLE, PROBE_LINEAR, PROBE_P2, PROBE_XOR_P2 = 0, 1, 2, 3
+SLOT_BYTES = {FMT_KV64: 16, FMT_TAGVAL16: 4, FMT_TAG16: 2}
+
+
+class LevelCfg(C.Structure):
+    _fields_ = [("nslots", C.c_uint64), ("bucket_size", C.c_uint32), ("max_probes", C.c_uint32),
+                ("scheme", C.c_uint32), ("probe", C.c_uint32)]
+
+
+class Cfg(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("partition", C.c_uint32), ("nlevels", C.c_uint32),
+                ("pad", C.c_uint32), ("lv", LevelCfg * 2)]
+
+
+_lib = None
+_refhost = None
+
+U64P = C.POINTER(C.c_uint64)
+U8P = C.POINTER(C.c_uint8)
+
+
+def build() -> None:
+    """Compile the C restatement (and the reference host pin when the reference is present)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        L.pgo_murmur64a.restype = C.c_uint64
+        L.pgo_murmur64a.argtypes = [C.c_void_p, C.c_int, C.c_uint64]
+        L.pgo_tag16.restype = C.c_uint64
+        L.pgo_tag16.argtypes = [C.c_uint64]
+        L.pgo_probe_values.restype = C.c_int
+        L.pgo_probe_values.argtypes = [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, U64P]
+        L.pgo_table_create.restype = C.c_void_p
+        L.pgo_table_create.argtypes = [C.POINTER(Cfg), C.c_uint64]
+        L.pgo_table_destroy.argtypes = [C.c_void_p]
+        L.pgo_table_clear.argtypes = [C.c_void_p]
+        for f in ("pgo_level_nbuckets", "pgo_level_bytes", "pgo_level_seed"):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_void_p, C.c_int]
+        L.pgo_level_data.restype = C.c_void_p
+        L.pgo_level_data.argtypes = [C.c_void_p, C.c_int]
+        L.pgo_insert.restype = C.c_int
+        L.pgo_insert.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
+        L.pgo_query.restype = C.c_int
+        L.pgo_query.argtypes = [C.c_void_p, C.c_uint64, U64P]
+        L.pgo_remove.restype = C.c_int
+        L.pgo_remove.argtypes = [C.c_void_p, C.c_uint64]
+        L.pgo_bulk_insert.restype = C.c_uint64
+        L.pgo_bulk_insert.argtypes = [C.c_void_p, U64P, U64P, C.c_uint64, U8P]
+        L.pgo_bulk_query.restype = C.c_uint64
+        L.pgo_bulk_query.argtypes = [C.c_void_p, U64P, C.c_uint64, U64P, U8P]
+        L.pgo_bulk_remove.restype = C.c_uint64
+        L.pgo_bulk_remove.argtypes = [C.c_void_p, U64P, C.c_uint64, U8P]
+        L.pgo_count_fill.restype = C.c_uint64
+        L.pgo_count_fill.argtypes = [C.c_void_p, C.c_int]
+        L.pgo_mt_bulk_insert.restype = C.c_uint64
+        L.pgo_mt_bulk_insert.argtypes = [C.c_void_p, U64P, U64P, C.c_uint64, U8P, C.c_int]
+        L.pgo_mt_bulk_query.restype = C.c_uint64
+        L.pgo_mt_bulk_query.argtypes = [C.c_void_p, U64P, C.c_uint64, U64P, U8P, C.c_int]
+        L.pgo_mt_bulk_remove.restype = C.c_uint64
+        L.pgo_mt_bulk_remove.argtypes = [C.c_void_p, U64P, C.c_uint64, U8P, C.c_int]
+        L.pgo_online_cores.restype = C.c_int
+        L.pgo_splitmix64_fill.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, U64P]
+        _lib = L
+    return _lib
+
+
+def refhost():
+    """The reference's own hash / probe code compiled for the host, or None."""
+    global _refhost
+    if _refhost is None and REFHOST_PATH.exists():
+        L = C.CDLL(str(REFHOST_PATH))
+        L.refh_murmur64a.restype = C.c_uint64
+        L.refh_murmur64a.argtypes = [C.c_uint64, C.c_uint64]
+        L.refh_probe_values.restype = C.c_int
+        L.refh_probe_values.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, U64P, C.c_int]
+        _refhost = L
+    return _refhost
+
+
+def _p64(a):
+    return None if a is None else a.ctypes.data_as(U64P)
+
+
+def _p8(a):
+    return None if a is None else a.ctypes.data_as(U8P)
+
+
+def splitmix64(seed: int, n: int, start: int = 0) -> np.ndarray:
+    out = np.empty(n, dtype=np.uint64)
+    lib().pgo_splitmix64_fill(seed, start, n, _p64(out))
+    return out
+
+
+def murmur64a(key: int, seed: int) -> int:
+    k = C.c_uint64(key)
+    return lib().pgo_murmur64a(C.byref(k), 8, seed)
+
+
+def probe_values(probe: int, seed: int, fmt: int, key: int, max_probes: int) -> list[int]:
+    out = np.zeros(max(max_probes, 1), dtype=np.uint64)
+    n = lib().pgo_probe_values(probe, seed, fmt, key, max_probes, _p64(out))
+    return [int(x) for x in out[:n]]
+
+
+def make_cfg(fmt: int, partition: int, levels: list[tuple]) -> Cfg:
+    """levels: [(nslots, bucket_size, max_probes, scheme, probe), ...]"""
+    c = Cfg()
+    c.format, c.partition, c.nlevels = fmt, partition, len(levels)
+    for i, lv in enumerate(levels):
+        c.lv[i] = LevelCfg(*lv)
+    return c
+
+
+class OracleTable:
+    """Sequential model of one reference table (static_table semantics)."""
+
+    def __init__(self, fmt: int, partition: int, levels: list[tuple], seed: int):
+        self.cfg = make_cfg(fmt, partition, levels)
+        self.fmt = fmt
+        self.h = lib().pgo_table_create(C.byref(self.cfg), seed)
+        if not self.h:
+            raise ValueError("invalid oracle table configuration")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().pgo_table_destroy(h)
+            self.h = None
+
+    @property
+    def nlevels(self) -> int:
+        return self.cfg.nlevels
+
+    def clear(self):
+        lib().pgo_table_clear(self.h)
+
+    def nbuckets(self, level: int) -> int:
+        return lib().pgo_level_nbuckets(self.h, level)
+
+    def level_bytes(self, level: int) -> bytes:
+        n = lib().pgo_level_bytes(self.h, level)
+        return C.string_at(lib().pgo_level_data(self.h, level), n)
+
+    def insert_many(self, keys, vals=None, threads: int | None = None):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        vals = None if vals is None else np.ascontiguousarray(vals, dtype=np.uint64)
+        ok = np.zeros(len(keys), dtype=np.uint8)
+        if threads is None:
+            lib().pgo_bulk_insert(self.h, _p64(keys), _p64(vals), len(keys), _p8(ok))
+        else:
+            lib().pgo_mt_bulk_insert(self.h, _p64(keys), _p64(vals), len(keys), _p8(ok), threads)
+        return ok.astype(bool)
+
+    def query_many(self, keys, threads: int | None = None):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        vals = np.zeros(len(keys), dtype=np.uint64)
+        found = np.zeros(len(keys), dtype=np.uint8)
+        if threads is None:
+            lib().pgo_bulk_query(self.h, _p64(keys), len(keys), _p64(vals), _p8(found))
+        else:
+            lib().pgo_mt_bulk_query(self.h, _p64(keys), len(keys), _p64(vals), _p8(found), threads)
+        return found.astype(bool), vals
+
+    def remove_many(self, keys, threads: int | None = None):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        ok = np.zeros(len(keys), dtype=np.uint8)
+        if threads is None:
+            lib().pgo_bulk_remove(self.h, _p64(keys), len(keys), _p8(ok))
+        else:
+            lib().pgo_mt_bulk_remove(self.h, _p64(keys), len(keys), _p8(ok), threads)
+        return ok.astype(bool)
+
+    def count_fill(self, level: int) -> int:
+        return lib().pgo_count_fill(self.h, level)
+
+
+def online_cores() -> int:
+    return lib().pgo_online_cores()

@@ -1,0 +1,328 @@
+"""poggers_b200 -- B200-native (sm_100a) POGGERS hot path.
+
+Python host API over the C ABI of libpoggers_b200.so (include/poggers_b200.h).
+Names follow the reference's template API so a reference user recognises
+them:
+
+    reference (C++ templates)                       here
+    poggers::tables::static_table<...>              Table(TableConfig, seed)
+    Table::generate_on_device(&sizing, seed)        Table.generate_on_device(config, sizing, seed)
+    Table::free_on_device(table)                    table.free_on_device()
+    insert / query / remove(tile, key[, val])       bulk_insert / bulk_query / bulk_remove
+    poggers::data_structs::tcf                      data_structs.tcf(...)
+    poggers::data_structs::hash_table_64            data_structs.hash_table_64(...)
+    poggers::sizing::size_in_num_slots<N>(...)      sizing.size_in_num_slots(...)
+
+Device buffers are torch CUDA tensors (or raw device addresses as ints).
+The library must be built (poggers_b200/build.py); nothing here falls back
+to a CPU path: a missing or unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libpoggers_b200.so"
+
+# ---- enums (include/poggers_b200.h)
+PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT = range(7)
+FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
+SCHEME_BUCKET, SCHEME_TWO_CHOICE = 0, 1
+PROBE_DOUBLE, PROBE_LINEAR, PROBE_P2, PROBE_XOR_P2 = 0, 1, 2, 3
+KEY_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 2}
+VAL_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 0}
+SLOT_BYTES = {f: KEY_BYTES[f] + VAL_BYTES[f] for f in KEY_BYTES}
+
+
+class PoggersError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+class _LevelConfig(C.Structure):
+    _fields_ = [("nslots", C.c_uint64), ("bucket_size", C.c_uint32), ("max_probes", C.c_uint32),
+                ("scheme", C.c_uint32), ("probe", C.c_uint32)]
+
+
+class _TableConfig(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("tile", C.c_uint32), ("nlevels", C.c_uint32),
+                ("reserved", C.c_uint32), ("levels", _LevelConfig * 2)]
+
+
+class _LevelInfo(C.Structure):
+    _fields_ = [("nbuckets", C.c_uint64), ("nslots", C.c_uint64), ("bytes", C.c_uint64),
+                ("seed", C.c_uint64), ("d_buckets", C.c_void_p)]
+
+
+_lib = None
+
+EXPORTED = (
+    "pg_version", "pg_status_string", "pg_table_create", "pg_table_destroy", "pg_table_clear",
+    "pg_table_level_info", "pg_table_bytes", "pg_table_set_launch", "pg_bulk_insert", "pg_bulk_query",
+    "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
+    "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
+)
+
+
+def lib() -> C.CDLL:
+    """Load libpoggers_b200.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python poggers_b200/build.py`")
+    L = C.CDLL(str(LIB_PATH))
+    V, P, U64, U32 = C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32
+    L.pg_version.restype = C.c_char_p
+    L.pg_status_string.restype = C.c_char_p
+    L.pg_status_string.argtypes = [C.c_int]
+    L.pg_table_create.restype = C.c_int
+    L.pg_table_create.argtypes = [C.POINTER(_TableConfig), U64, C.POINTER(V)]
+    L.pg_table_destroy.restype = C.c_int
+    L.pg_table_destroy.argtypes = [V]
+    L.pg_table_clear.restype = C.c_int
+    L.pg_table_clear.argtypes = [V, P]
+    L.pg_table_level_info.restype = C.c_int
+    L.pg_table_level_info.argtypes = [V, U32, C.POINTER(_LevelInfo)]
+    L.pg_table_bytes.restype = U64
+    L.pg_table_bytes.argtypes = [V]
+    L.pg_table_set_launch.restype = C.c_int
+    L.pg_table_set_launch.argtypes = [V, U32, U32, U32]
+    L.pg_bulk_insert.restype = C.c_int
+    L.pg_bulk_insert.argtypes = [V, P, P, U64, P, P, P]
+    L.pg_bulk_query.restype = C.c_int
+    L.pg_bulk_query.argtypes = [V, P, U64, P, P, P, P]
+    L.pg_bulk_remove.restype = C.c_int
+    L.pg_bulk_remove.argtypes = [V, P, U64, P, P, P]
+    L.pg_table_count_fill.restype = C.c_int
+    L.pg_table_count_fill.argtypes = [V, U32, P, P]
+    L.pg_table_dump_level.restype = C.c_int
+    L.pg_table_dump_level.argtypes = [V, U32, P, U64]
+    L.pg_table_load_level.restype = C.c_int
+    L.pg_table_load_level.argtypes = [V, U32, P, U64]
+    L.pg_host_murmur64a.restype = U64
+    L.pg_host_murmur64a.argtypes = [U64, U64]
+    L.pg_host_fastmod.restype = U64
+    L.pg_host_fastmod.argtypes = [U64, U64]
+    L.pg_host_probe_buckets.restype = U32
+    L.pg_host_probe_buckets.argtypes = [C.POINTER(_TableConfig), U32, U64, U64, C.POINTER(U64), U32]
+    _lib = L
+    return L
+
+
+def version() -> str:
+    return lib().pg_version().decode()
+
+
+def status_string(s: int) -> str:
+    return lib().pg_status_string(s).decode()
+
+
+def _check(st: int, what: str) -> None:
+    if st != PG_OK:
+        raise PoggersError(st, what)
+
+
+def _ptr(x) -> int | None:
+    """Device address of a torch tensor / int / None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _stream(s) -> int | None:
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+# ---------------------------------------------------------------- configs
+@dataclass
+class Level:
+    nslots: int
+    bucket_size: int
+    max_probes: int
+    scheme: int = SCHEME_BUCKET
+    probe: int = PROBE_DOUBLE
+
+
+@dataclass
+class TableConfig:
+    format: int
+    tile: int
+    levels: list[Level] = field(default_factory=list)
+
+    def c(self) -> _TableConfig:
+        c = _TableConfig()
+        c.format, c.tile, c.nlevels, c.reserved = self.format, self.tile, len(self.levels), 0
+        for i, L in enumerate(self.levels):
+            c.levels[i] = _LevelConfig(L.nslots, L.bucket_size, L.max_probes, L.scheme, L.probe)
+        return c
+
+    def with_sizes(self, *nslots: int) -> "TableConfig":
+        if len(nslots) != len(self.levels):
+            raise ValueError("sizing lists one slot count per level")
+        return TableConfig(self.format, self.tile,
+                           [Level(n, L.bucket_size, L.max_probes, L.scheme, L.probe)
+                            for n, L in zip(nslots, self.levels)])
+
+
+class sizing:
+    """poggers::sizing::size_in_num_slots<N>: one slot count per table level."""
+
+    class size_in_num_slots:
+        def __init__(self, *nslots: int):
+            self.nslots = tuple(int(n) for n in nslots)
+
+        def total(self) -> int:
+            return sum(self.nslots)
+
+
+# ---------------------------------------------------------------- table
+class Table:
+    """One device-resident table (static_table with an optional backing level)."""
+
+    def __init__(self, config: TableConfig, seed: int):
+        self.config = config
+        self.seed = seed
+        self._c = config.c()
+        h = C.c_void_p()
+        _check(lib().pg_table_create(C.byref(self._c), seed, C.byref(h)), "pg_table_create")
+        self._h = h
+
+    @classmethod
+    def generate_on_device(cls, config: TableConfig, sizing_obj: "sizing.size_in_num_slots", seed: int) -> "Table":
+        """static_table::generate_on_device(Sizing*, seed): raises ValueError when the
+        sizing lists a different number of levels (base_table.cuh:116-131)."""
+        return cls(config.with_sizes(*sizing_obj.nslots), seed)
+
+    def free_on_device(self) -> None:
+        if getattr(self, "_h", None):
+            _check(lib().pg_table_destroy(self._h), "pg_table_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free_on_device()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def format(self) -> int:
+        return self.config.format
+
+    def clear(self, stream=None) -> None:
+        _check(lib().pg_table_clear(self._h, _stream(stream)), "pg_table_clear")
+
+    def set_launch(self, block_threads: int = 0, blocks_per_sm: int = 0, max_blocks: int = 0) -> None:
+        _check(lib().pg_table_set_launch(self._h, block_threads, blocks_per_sm, max_blocks), "pg_table_set_launch")
+
+    def serial(self) -> None:
+        """One group walks the batch in order (deterministic layout, for parity checks)."""
+        self.set_launch(self.config.tile, 1, 1)
+
+    def level_info(self, level: int) -> dict:
+        info = _LevelInfo()
+        _check(lib().pg_table_level_info(self._h, level, C.byref(info)), "pg_table_level_info")
+        return {"nbuckets": info.nbuckets, "nslots": info.nslots, "bytes": info.bytes, "seed": info.seed,
+                "d_buckets": info.d_buckets}
+
+    def host_bytes_in_use(self) -> int:
+        return lib().pg_table_bytes(self._h)
+
+    def bulk_insert(self, keys, vals=None, ok=None, fail_count=None, stream=None, n: int | None = None) -> None:
+        n = keys.numel() if n is None else n
+        _check(lib().pg_bulk_insert(self._h, _ptr(keys), _ptr(vals), n, _ptr(ok), _ptr(fail_count),
+                                    _stream(stream)), "pg_bulk_insert")
+
+    def bulk_query(self, keys, vals_out=None, found=None, hit_count=None, stream=None, n: int | None = None) -> None:
+        n = keys.numel() if n is None else n
+        _check(lib().pg_bulk_query(self._h, _ptr(keys), n, _ptr(vals_out), _ptr(found), _ptr(hit_count),
+                                   _stream(stream)), "pg_bulk_query")
+
+    def bulk_remove(self, keys, ok=None, hit_count=None, stream=None, n: int | None = None) -> None:
+        n = keys.numel() if n is None else n
+        _check(lib().pg_bulk_remove(self._h, _ptr(keys), n, _ptr(ok), _ptr(hit_count), _stream(stream)),
+               "pg_bulk_remove")
+
+    def count_fill(self, level: int, out, stream=None) -> None:
+        """out (2 x uint64 device) += [occupied slots, tombstones] of `level`."""
+        _check(lib().pg_table_count_fill(self._h, level, _ptr(out), _stream(stream)), "pg_table_count_fill")
+
+    def get_fill(self, level: int = 0) -> tuple[int, int]:
+        import torch
+        out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        self.count_fill(level, out)
+        torch.cuda.synchronize()
+        return int(out[0]), int(out[1])
+
+    def dump_level(self, level: int) -> bytes:
+        info = self.level_info(level)
+        nbytes = info["nslots"] * SLOT_BYTES[self.format]
+        buf = C.create_string_buffer(nbytes)
+        _check(lib().pg_table_dump_level(self._h, level, buf, nbytes), "pg_table_dump_level")
+        return buf.raw
+
+    def load_level(self, level: int, data: bytes) -> None:
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(lib().pg_table_load_level(self._h, level, buf, len(data)), "pg_table_load_level")
+
+
+# ---------------------------------------------------------------- named tables
+class data_structs:
+    """The reference's public aliases (include/poggers/data_structs/) as configurations."""
+
+    @staticmethod
+    def tiny_static_table_4(nslots: int) -> TableConfig:
+        # static_table<uint64,uint16,dynamic_container<key_val_pair,uint16>,4,4,bucket_insert,20,doubleHasher>
+        return TableConfig(FMT_TAGVAL16, 4, [Level(nslots, 4, 20, SCHEME_BUCKET, PROBE_DOUBLE)])
+
+    @staticmethod
+    def tcf(nslots: int, backing_nslots: int, tile: int = 4, bucket: int = 16) -> TableConfig:
+        # data_structs/tcf.cuh:30: two-choice shortcut over 16-slot buckets, 2 double-hash probes,
+        # backed by tiny_static_table_4
+        return TableConfig(FMT_TAGVAL16, tile, [Level(nslots, bucket, 2, SCHEME_TWO_CHOICE, PROBE_DOUBLE),
+                                                Level(backing_nslots, 4, 20, SCHEME_BUCKET, PROBE_DOUBLE)])
+
+    @staticmethod
+    def tcqf(nslots: int, tile: int = 4, bucket: int = 16) -> TableConfig:
+        # tag-only filter: dynamic_container<key_container,uint16> two-choice, no backing
+        # (tests/src/bucket_speed_tests.cu:108, tcqf_16_16)
+        return TableConfig(FMT_TAG16, tile, [Level(nslots, bucket, 2, SCHEME_TWO_CHOICE, PROBE_DOUBLE)])
+
+    @staticmethod
+    def hash_table_64(nslots: int, tile: int = 4, bucket: int = 16, probe: int = PROBE_DOUBLE,
+                      max_probes: int = 20) -> TableConfig:
+        # data_structs/uint64_hash_table.cuh:35
+        return TableConfig(FMT_KV64, tile, [Level(nslots, bucket, max_probes, SCHEME_BUCKET, probe)])
+
+    @staticmethod
+    def two_choice_table_64(nslots: int, tile: int = 4, bucket: int = 8) -> TableConfig:
+        # static_table<uint64,uint64,key_val_pair,4,B,power_of_n_insert_shortcut_scheme,2,powerOfTwoHasher>
+        return TableConfig(FMT_KV64, tile, [Level(nslots, bucket, 2, SCHEME_TWO_CHOICE, PROBE_P2)])
+
+
+def host_murmur64a(key: int, seed: int) -> int:
+    return lib().pg_host_murmur64a(key, seed)
+
+
+def host_fastmod(n: int, d: int) -> int:
+    return lib().pg_host_fastmod(n, d)
+
+
+def host_probe_buckets(config: TableConfig, level: int, seed: int, key: int) -> list[int]:
+    out = (C.c_uint64 * 64)()
+    c = config.c()
+    n = lib().pg_host_probe_buckets(C.byref(c), level, seed, key, out, 64)
+    return list(out[:n])

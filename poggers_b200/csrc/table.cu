@@ -1,0 +1,358 @@
+// table.cu -- C ABI: table lifetime, bulk-op launchers, fill counts, dumps.
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <cuda_runtime.h>
+#include <vector>
+
+#include "poggers_b200.h"
+#include "bulk_kernels.cuh"
+
+using namespace pg;
+
+struct pg_table {
+    pg_table_config cfg;
+    table_desc desc;
+    void *mem[2];
+    uint64_t bytes[2];
+    int device;
+    int num_sms;
+    uint32_t block_threads;
+    uint32_t blocks_per_sm;
+    uint32_t max_blocks;
+};
+
+namespace {
+
+uint32_t key_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : 2u; }
+uint32_t val_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : (fmt == PG_FMT_TAGVAL16 ? 2u : 0u); }
+
+pg_status validate(const pg_table_config *c)
+{
+    if (!c || c->reserved != 0) return PG_ERR_INVALID;
+    if (c->format > PG_FMT_TAG16) return PG_ERR_INVALID;
+    if (c->nlevels < 1 || c->nlevels > 2) return PG_ERR_INVALID;
+    if (!(c->tile == 1 || c->tile == 2 || c->tile == 4 || c->tile == 8 || c->tile == 16)) return PG_ERR_INVALID;
+    for (uint32_t l = 0; l < c->nlevels; l++) {
+        const pg_level_config &L = c->levels[l];
+        if (L.nslots == 0 || L.bucket_size == 0 || L.max_probes == 0) return PG_ERR_INVALID;
+        if (L.scheme > PG_SCHEME_TWO_CHOICE || L.probe > PG_PROBE_XOR_P2) return PG_ERR_INVALID;
+        if ((L.probe == PG_PROBE_P2 || L.probe == PG_PROBE_XOR_P2) && L.max_probes != 2) return PG_ERR_INVALID;
+        if (L.scheme == PG_SCHEME_TWO_CHOICE && L.max_probes > (uint32_t)kTwoChoiceMaxProbes) return PG_ERR_UNSUPPORTED;
+        if (L.bucket_size > 64) return PG_ERR_UNSUPPORTED;
+        if (L.nslots / L.bucket_size > (1ULL << 40)) return PG_ERR_INVALID;
+    }
+    const uint32_t b0 = c->levels[0].bucket_size;
+    if (!(b0 == 4 || b0 == 8 || b0 == 16 || b0 == 32)) return PG_ERR_UNSUPPORTED;
+    if (c->tile > b0) return PG_ERR_UNSUPPORTED;
+    return PG_OK;
+}
+
+pg_status cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return PG_OK;
+    if (e == cudaErrorMemoryAllocation) return PG_ERR_NOMEM;
+    if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;
+    return PG_ERR_CUDA;
+}
+
+void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block)
+{
+    const uint32_t bt = t->block_threads;
+    const uint64_t groups_per_block = bt / t->cfg.tile;
+    uint64_t need = (n + groups_per_block - 1) / groups_per_block;
+    uint64_t cap = (uint64_t)t->num_sms * t->blocks_per_sm;
+    if (t->max_blocks && cap > t->max_blocks) cap = t->max_blocks;
+    if (need > cap) need = cap;
+    if (need == 0) need = 1;
+    grid = dim3((unsigned)need);
+    block = dim3(bt);
+}
+
+pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
+{
+    if (!t) return PG_ERR_INVALID;
+    if (a.n == 0) return PG_OK;
+    if (!a.keys) return PG_ERR_INVALID;
+    dim3 grid, block;
+    launch_shape(t, a.n, grid, block);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t b0 = t->cfg.levels[0].bucket_size, tile = t->cfg.tile;
+    cudaError_t e;
+    switch (t->cfg.format) {
+    case PG_FMT_KV64: e = launch_kv64(op, b0, tile, t->desc, a, grid, block, s); break;
+    case PG_FMT_TAGVAL16: e = launch_tagval16(op, b0, tile, t->desc, a, grid, block, s); break;
+    default: e = launch_tag16(op, b0, tile, t->desc, a, grid, block, s); break;
+    }
+    return cuda_status(e);
+}
+
+// occupied / tombstone counts of one level: one thread per bucket
+template <class K>
+__global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, uint64_t nb, uint32_t B,
+                                                    uint32_t bucket_bytes, K tomb, unsigned long long *out)
+{
+    uint32_t occ = 0, tmb = 0;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (uint64_t)gridDim.x * blockDim.x) {
+        const K *k = reinterpret_cast<const K *>(base + b * bucket_bytes);
+        for (uint32_t s = 0; s < B; s++) {
+            K v = __ldcs(k + s);
+            occ += v != (K)0;
+            tmb += v == tomb;
+        }
+    }
+    __shared__ unsigned int sh[2];
+    if (threadIdx.x == 0) sh[0] = sh[1] = 0;
+    __syncthreads();
+    unsigned am = __activemask();
+    unsigned so = __reduce_add_sync(am, occ), st = __reduce_add_sync(am, tmb);
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&sh[0], so);
+        atomicAdd(&sh[1], st);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sh[0]) atomicAdd(out, (unsigned long long)sh[0]);
+        if (sh[1]) atomicAdd(out + 1, (unsigned long long)sh[1]);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pg_version(void) { return "poggers_b200 0.1 sm_100a"; }
+
+const char *pg_status_string(pg_status s)
+{
+    switch (s) {
+    case PG_OK: return "ok";
+    case PG_ERR_INVALID: return "invalid argument";
+    case PG_ERR_CUDA: return "CUDA error";
+    case PG_ERR_NOMEM: return "out of device memory";
+    case PG_ERR_UNSUPPORTED: return "unsupported configuration";
+    case PG_ERR_FULL: return "capacity exhausted";
+    case PG_ERR_TIMEOUT: return "bounded device wait timed out";
+    }
+    return "unknown status";
+}
+
+pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **out)
+{
+    if (!out) return PG_ERR_INVALID;
+    *out = nullptr;
+    pg_status st = validate(cfg);
+    if (st != PG_OK) return st;
+    pg_table *t = (pg_table *)calloc(1, sizeof(pg_table));
+    if (!t) return PG_ERR_NOMEM;
+    t->cfg = *cfg;
+    if (cudaGetDevice(&t->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, t->device) != cudaSuccess) {
+        free(t);
+        return PG_ERR_CUDA;
+    }
+    t->block_threads = 256;
+    t->blocks_per_sm = 8;
+    t->max_blocks = 0;
+    t->desc.nlevels = cfg->nlevels;
+    t->desc.format = cfg->format;
+    const uint32_t kb = key_bytes(cfg->format), vb = val_bytes(cfg->format);
+    uint64_t s = seed;
+    for (uint32_t l = 0; l < cfg->nlevels; l++) {
+        const pg_level_config &L = cfg->levels[l];
+        level_desc &D = t->desc.lv[l];
+        const uint64_t nb = (L.nslots - 1) / L.bucket_size + 1;  // min_buckets, bucket_insert.cuh:90
+        D.bucket_size = L.bucket_size;
+        D.max_probes = L.max_probes;
+        D.scheme = L.scheme;
+        D.probe = L.probe;
+        D.bucket_bytes = L.bucket_size * (kb + vb);
+        D.val_offset = L.bucket_size * kb;
+        D.nbmod = make_fastmod64(nb);
+        D.seed = s;
+        D.seed2 = s * s;
+        t->bytes[l] = nb * D.bucket_bytes;
+        cudaError_t e = cudaMalloc(&t->mem[l], t->bytes[l]);
+        if (e == cudaSuccess) e = cudaMemset(t->mem[l], 0, t->bytes[l]);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            for (uint32_t j = 0; j <= l; j++)
+                if (t->mem[j]) cudaFree(t->mem[j]);
+            free(t);
+            return cuda_status(e);
+        }
+        D.base = static_cast<unsigned char *>(t->mem[l]);
+        s = s * s;  // recursive table gets seed*seed (base_table.cuh:124)
+    }
+    *out = t;
+    return PG_OK;
+}
+
+pg_status pg_table_destroy(pg_table *t)
+{
+    if (!t) return PG_ERR_INVALID;
+    pg_status st = PG_OK;
+    for (int l = 0; l < 2; l++)
+        if (t->mem[l] && cudaFree(t->mem[l]) != cudaSuccess) st = PG_ERR_CUDA;
+    free(t);
+    return st;
+}
+
+pg_status pg_table_clear(pg_table *t, pg_stream_t stream)
+{
+    if (!t) return PG_ERR_INVALID;
+    for (uint32_t l = 0; l < t->cfg.nlevels; l++) {
+        cudaError_t e = cudaMemsetAsync(t->mem[l], 0, t->bytes[l], reinterpret_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return PG_OK;
+}
+
+pg_status pg_table_level_info(const pg_table *t, uint32_t level, pg_level_info *out)
+{
+    if (!t || !out || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    const level_desc &D = t->desc.lv[level];
+    out->nbuckets = D.nbmod.d;
+    out->nslots = D.nbmod.d * D.bucket_size;
+    out->bytes = t->bytes[level];
+    out->seed = D.seed;
+    out->d_buckets = t->mem[level];
+    return PG_OK;
+}
+
+uint64_t pg_table_bytes(const pg_table *t)
+{
+    if (!t) return 0;
+    return t->bytes[0] + t->bytes[1];
+}
+
+pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks)
+{
+    if (!t) return PG_ERR_INVALID;
+    if (block_threads == 0) block_threads = 256;
+    if (blocks_per_sm == 0) blocks_per_sm = 8;
+    if (block_threads > 256 || block_threads % t->cfg.tile != 0) return PG_ERR_INVALID;
+    if (block_threads < 32 && max_blocks != 1) return PG_ERR_INVALID;  // partial warps only for the serial shape
+    t->block_threads = block_threads;
+    t->blocks_per_sm = blocks_per_sm;
+    t->max_blocks = max_blocks;
+    return PG_OK;
+}
+
+pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n, uint8_t *d_ok,
+                         uint64_t *d_fail_count, pg_stream_t stream)
+{
+    bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
+                reinterpret_cast<unsigned long long *>(d_fail_count), n};
+    return run_bulk(t, OP_INSERT, a, stream);
+}
+
+pg_status pg_bulk_query(pg_table *t, const uint64_t *d_keys, uint64_t n, void *d_vals_out, uint8_t *d_found,
+                        uint64_t *d_hit_count, pg_stream_t stream)
+{
+    bulk_args a{d_keys, nullptr, d_vals_out, d_found, reinterpret_cast<unsigned long long *>(d_hit_count), n};
+    return run_bulk(t, OP_QUERY, a, stream);
+}
+
+pg_status pg_bulk_remove(pg_table *t, const uint64_t *d_keys, uint64_t n, uint8_t *d_ok, uint64_t *d_hit_count,
+                         pg_stream_t stream)
+{
+    bulk_args a{d_keys, nullptr, nullptr, d_ok, reinterpret_cast<unsigned long long *>(d_hit_count), n};
+    return run_bulk(t, OP_REMOVE, a, stream);
+}
+
+pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_stream_t stream)
+{
+    if (!t || !d_out || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    const level_desc &D = t->desc.lv[level];
+    const uint64_t nb = D.nbmod.d;
+    uint64_t blocks = (nb + 255) / 256;
+    uint64_t cap = (uint64_t)t->num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    auto *out = reinterpret_cast<unsigned long long *>(d_out);
+    if (t->cfg.format == PG_FMT_KV64)
+        k_count_fill<unsigned long long><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
+                                                                          ~0ULL, out);
+    else
+        k_count_fill<unsigned short><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
+                                                                      (unsigned short)0xFFFFu, out);
+    return cuda_status(cudaGetLastError());
+}
+
+// Reference slot layout: slot s of bucket b at (b*B + s) * slot_bytes, the
+// key first, then the val (key_val_pair.cuh:72-74); tag-only slots hold the key.
+pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst, uint64_t bytes)
+{
+    if (!t || !host_dst || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    const level_desc &D = t->desc.lv[level];
+    const uint32_t kb = key_bytes(t->cfg.format), vb = val_bytes(t->cfg.format), sb = kb + vb;
+    const uint64_t nslots = D.nbmod.d * D.bucket_size;
+    if (bytes != nslots * sb) return PG_ERR_INVALID;
+    std::vector<unsigned char> raw(t->bytes[level]);
+    cudaError_t e = cudaMemcpy(raw.data(), t->mem[level], t->bytes[level], cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e);
+    unsigned char *dst = static_cast<unsigned char *>(host_dst);
+    const uint32_t B = D.bucket_size;
+    for (uint64_t b = 0; b < D.nbmod.d; b++) {
+        const unsigned char *src = raw.data() + b * D.bucket_bytes;
+        for (uint32_t s = 0; s < B; s++) {
+            unsigned char *slot = dst + (b * B + s) * sb;
+            memcpy(slot, src + s * kb, kb);
+            if (vb) memcpy(slot + kb, src + D.val_offset + s * vb, vb);
+        }
+    }
+    return PG_OK;
+}
+
+pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes)
+{
+    if (!t || !host_src || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    const level_desc &D = t->desc.lv[level];
+    const uint32_t kb = key_bytes(t->cfg.format), vb = val_bytes(t->cfg.format), sb = kb + vb;
+    const uint64_t nslots = D.nbmod.d * D.bucket_size;
+    if (bytes != nslots * sb) return PG_ERR_INVALID;
+    std::vector<unsigned char> raw(t->bytes[level]);
+    const unsigned char *src = static_cast<const unsigned char *>(host_src);
+    const uint32_t B = D.bucket_size;
+    for (uint64_t b = 0; b < D.nbmod.d; b++) {
+        unsigned char *dst = raw.data() + b * D.bucket_bytes;
+        for (uint32_t s = 0; s < B; s++) {
+            const unsigned char *slot = src + (b * B + s) * sb;
+            memcpy(dst + s * kb, slot, kb);
+            if (vb) memcpy(dst + D.val_offset + s * vb, slot + kb, vb);
+        }
+    }
+    return cuda_status(cudaMemcpy(t->mem[level], raw.data(), t->bytes[level], cudaMemcpyHostToDevice));
+}
+
+uint64_t pg_host_murmur64a(uint64_t key, uint64_t seed) { return murmur64a_u64(key, seed); }
+
+uint64_t pg_host_fastmod(uint64_t n, uint64_t d)
+{
+    if (d == 0) return 0;
+    return make_fastmod64(d).mod(n);
+}
+
+uint32_t pg_host_probe_buckets(const pg_table_config *cfg, uint32_t level, uint64_t seed, uint64_t key, uint64_t *out,
+                               uint32_t cap)
+{
+    if (validate(cfg) != PG_OK || level >= cfg->nlevels || !out) return 0;
+    uint64_t s = seed;
+    for (uint32_t l = 0; l < level; l++) s = s * s;
+    const pg_level_config &L = cfg->levels[level];
+    const uint64_t nb = (L.nslots - 1) / L.bucket_size + 1;
+    const fastmod64 fm = make_fastmod64(nb);
+    const uint64_t tag = cfg->format == PG_FMT_KV64 ? key : tag16(key);
+    probe_seq ps;
+    ps.begin(L.probe, key, tag, s, s * s);
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < L.max_probes && n < cap; i++) {
+        uint64_t raw = ps.at(i);
+        if (raw == kProbeEnd) break;
+        out[n++] = fm.mod(raw);
+    }
+    return n;
+}
+
+}  // extern "C"

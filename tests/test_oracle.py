@@ -1,0 +1,167 @@
+"""CPU tests: the oracle pinned to the reference, and oracle semantics.
+
+The oracle's hashing and probing are checked bit for bit against the
+reference's own code compiled for the host (oracle/_ref/libpoggers_refhost.so);
+its table model is checked byte for byte against golden dumps recorded from
+the reference's CUDA build (tests/golden/).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tests.cases import CASES, golden, oracle_table
+from poggers_b200 import workload as wl
+
+
+def test_splitmix_matches_numpy(oracle):
+    a = oracle.splitmix64(42, 10000)
+    b = wl.splitmix64(42, 10000)
+    assert (a == b).all()
+    assert len(np.unique(a)) == len(a)
+
+
+def test_murmur_pinned_to_reference(oracle):
+    rh = oracle.refhost()
+    if rh is None:
+        pytest.skip("reference host build absent (make -C oracle ref)")
+    keys = list(map(int, wl.splitmix64(1, 3000))) + [0, 1, (1 << 64) - 1, 0x8000000000000000]
+    for s in (42, 43, 42 * 42, (42 ** 4) % (1 << 64), 0, (1 << 64) - 1):
+        for k in keys:
+            assert oracle.murmur64a(k, s) == rh.refh_murmur64a(k, s)
+
+
+@pytest.mark.parametrize("kind,maxp", [(0, 20), (1, 20), (2, 2), (3, 2)])
+def test_probe_sequences_pinned_to_reference(oracle, kind, maxp):
+    rh = oracle.refhost()
+    if rh is None:
+        pytest.skip("reference host build absent (make -C oracle ref)")
+    for fmt in (0, 1):
+        for k in map(int, wl.splitmix64(7 + kind, 2000)):
+            tag = k if fmt == 0 else int(oracle.lib().pgo_tag16(k))
+            ref = (C.c_uint64 * 32)()
+            n = rh.refh_probe_values(kind, 42, k, tag, ref, 32)
+            assert list(ref[:n]) == oracle.probe_values(kind, 42, fmt, k, maxp)
+
+
+def test_tag16_remaps_sentinels(oracle):
+    t = oracle.lib().pgo_tag16
+    assert t(0) == 1 and t(0x10000) == 1
+    assert t(0xFFFF) == 0xFFFE and t(0xABCD0000FFFF) == 0xFFFE
+    assert t(0x1234) == 0x1234
+
+
+def _replay(oracle, name, g, partition=None):
+    t = oracle_table(oracle, name, partition)
+    ok = t.insert_many(g["keys"], g["vals"])
+    dumps = [t.level_bytes(l) for l in range(t.nlevels)]
+    qf, qv = t.query_many(g["qkeys"])
+    rok = t.remove_many(g["rkeys"])
+    dumps2 = [t.level_bytes(l) for l in range(t.nlevels)]
+    qf2, qv2 = t.query_many(g["qkeys"])
+    return ok, dumps, qf, qv, rok, dumps2, qf2, qv2
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_golden(oracle, name):
+    g = golden(name)
+    if g is None:
+        pytest.skip(f"golden fixture ref_{name}.npz not recorded yet")
+    ok, dumps, qf, qv, rok, dumps2, qf2, qv2 = _replay(oracle, name, g)
+    assert (ok == g["insert_ok"].astype(bool)).all()
+    for l, d in enumerate(dumps):
+        assert d == g[f"dump_insert_l{l}"].tobytes(), f"level {l} layout after inserts"
+    assert (qf == g["q_found"].astype(bool)).all()
+    assert (qv == g["q_vals"]).all()
+    assert (rok == g["remove_ok"].astype(bool)).all()
+    for l, d in enumerate(dumps2):
+        assert d == g[f"dump_remove_l{l}"].tobytes(), f"level {l} layout after removes"
+    assert (qf2 == g["q2_found"].astype(bool)).all()
+    assert (qv2 == g["q2_vals"]).all()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tile_width_does_not_change_results(oracle, name):
+    """Filled slots form a prefix of each bucket, so the reference's stripe width
+    (Partition_Size) never changes a result of phase-separated operations."""
+    fmt, tile, levels, seed = CASES[name]
+    keys = np.concatenate([wl.keys_without_sentinels(99, 1500), np.array([0, (1 << 64) - 1], dtype=np.uint64)])
+    g = {"keys": keys, "vals": wl.values_for(keys, 8, 3).astype(np.uint64),
+         "qkeys": np.concatenate([keys, wl.keys_without_sentinels(98, 300)]), "rkeys": keys[:400]}
+    if fmt != 0:
+        g["vals"] &= np.uint64(0xFFFF)
+    base = _replay(oracle, name, g, partition=1)
+    for p in (2, 4):
+        other = _replay(oracle, name, g, partition=p)
+        for a, b in zip(base, other):
+            if isinstance(a, list):
+                assert a == b
+            else:
+                assert (a == b).all()
+
+
+def test_sentinel_semantics_ht(oracle):
+    """key 0 is the empty key and ~0 the tombstone of key_val_pair<uint64,uint64>:
+    inserting 0 writes a value into an empty slot without claiming it; querying 0
+    reports the first empty slot; removing 0 turns an empty slot into a tombstone."""
+    t = oracle.OracleTable(0, 4, [(64, 8, 20, 0, 0)], 5)
+    assert t.insert_many(np.array([0], dtype=np.uint64), np.array([77], dtype=np.uint64)).all()
+    assert t.count_fill(0) == 0
+    f, v = t.query_many(np.array([0], dtype=np.uint64))
+    assert f[0] and v[0] == 77
+    assert t.remove_many(np.array([0], dtype=np.uint64)).all()
+    assert t.count_fill(0) == 1
+    f, v = t.query_many(np.array([0], dtype=np.uint64))
+    assert f[0] and v[0] == 0  # the next empty slot of the same bucket
+
+
+def test_duplicate_keys_take_two_slots_and_query_returns_first(oracle):
+    t = oracle.OracleTable(0, 4, [(64, 8, 20, 0, 0)], 5)
+    k = np.array([12345, 12345], dtype=np.uint64)
+    assert t.insert_many(k, np.array([1, 2], dtype=np.uint64)).all()
+    assert t.count_fill(0) == 2
+    f, v = t.query_many(k[:1])
+    assert f[0] and v[0] == 1
+    assert t.remove_many(k[:1]).all()
+    f, v = t.query_many(k[:1])
+    assert f[0] and v[0] == 2
+
+
+def test_full_table_reports_failures(oracle):
+    t = oracle.OracleTable(0, 4, [(64, 8, 20, 0, 0)], 5)
+    keys = wl.keys_without_sentinels(3, 200)
+    ok = t.insert_many(keys)
+    assert ok.sum() <= 64 and (~ok).sum() >= 136
+    f, _ = t.query_many(keys)
+    assert (f == ok).all()
+
+
+def test_multithreaded_port_matches_sequential_ht(oracle):
+    keys = wl.keys_without_sentinels(11, 90000)
+    vals = wl.values_for(keys, 8, 12)
+    q = np.concatenate([keys[:45000], wl.keys_without_sentinels(13, 45000)])
+    seq = oracle.OracleTable(0, 4, [(100000, 8, 20, 0, 0)], 43)
+    mt = oracle.OracleTable(0, 4, [(100000, 8, 20, 0, 0)], 43)
+    ok_s = seq.insert_many(keys, vals)
+    ok_m = mt.insert_many(keys, vals, threads=4)
+    # at 0.9 load a handful of inserts fail; which ones depends on the order
+    assert (~ok_s).sum() < 20 and (~ok_m).sum() < 20
+    both = np.concatenate([ok_s[:45000] & ok_m[:45000], np.ones(45000, dtype=bool)])
+    a = seq.query_many(q)
+    b = mt.query_many(q, threads=4)
+    assert (a[0][both] == b[0][both]).all() and (a[1][both] == b[1][both]).all()
+    assert (b[0][:45000] == ok_m[:45000]).all()
+    ridx = wl.fisher_yates_half(len(keys), 5)
+    rs, rm = seq.remove_many(keys[ridx]), mt.remove_many(keys[ridx], threads=4)
+    assert (rs == ok_s[ridx]).all() and (rm == ok_m[ridx]).all()
+    a = seq.query_many(q)
+    b = mt.query_many(q, threads=4)
+    assert (a[0][both] == b[0][both]).all() and (a[1][both] == b[1][both]).all()
+
+
+def test_multithreaded_port_tcf_no_false_negatives(oracle):
+    keys = wl.keys_without_sentinels(21, 50000)
+    t = oracle.OracleTable(1, 4, [(1 << 16, 16, 2, 1, 0), ((1 << 16) // 100, 4, 20, 0, 0)], 42)
+    ok = t.insert_many(keys, wl.values_for(keys, 2, 1).astype(np.uint64), threads=4)
+    f, _ = t.query_many(keys, threads=4)
+    assert (f | ~ok).all()
