@@ -192,7 +192,7 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     rem_ms = e0.elapsed_time(e1)
 
-    e2e = run_e2e(args, table, keys, vals, qkeys, dev, world)
+    e2e = None if args.no_e2e else run_e2e(args, table, keys, vals, qkeys, dev, world)
 
     ops = (n + nq) * args.steps * world
     value = ops / (ms_max / 1e3) / 1e6
@@ -441,7 +441,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-target", choices=["cpu", "cuda"], default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--slots-log2", type=int, default=26,
+                    help="table size (default 26 = the benchmark workload; smaller only for profiling captures)")
     args = ap.parse_args()
+    global NSLOTS, WORKLOAD
+    if args.slots_log2 != 26:
+        NSLOTS = 1 << args.slots_log2
+        WORKLOAD = WORKLOAD.replace("2^26", f"2^{args.slots_log2}")
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     world = int(os.environ.get("WORLD_SIZE", "1"))

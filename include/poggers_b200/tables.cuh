@@ -1,0 +1,318 @@
+// tables.cuh -- the reference's template table API, implemented on the
+// poggers_b200 bucket kernels.  Device code written against
+//     poggers::tables::static_table<Key, Val, Rep, Partition_Size, Bucket_Size,
+//                                   Insert_Scheme, Max_Probes, Probing_Scheme,
+//                                   Hasher, Is_Recursive, Recursive_Type>
+// (include/poggers/tables/base_table.cuh:52-356) compiles against
+// poggers_b200::tables::static_table with the same template arguments, the
+// same host calls (generate_on_device(Sizing*, seed) returning a device
+// pointer, free_on_device, get_block_size, get_num_blocks, host_bytes_in_use)
+// and the same device calls on a cooperative-groups tile (insert, query,
+// remove, get_my_tile).  Tables are created through the C ABI
+// (pg_table_create), so a table made here can also be driven by the bulk
+// entry points.
+//
+// Supported instantiations (what the hot path uses): Key = uint64_t;
+//   Rep key_val_pair with Val = uint64_t                 -> uint64 hash tables
+//   Rep dynamic_container<key_val_pair, uint16_t>        -> TCF (16-bit tag + val)
+//   Rep dynamic_container<key_container, uint16_t>       -> tag-only TCF
+// Insert_Scheme bucket_insert or power_of_n_insert_shortcut_scheme; Probing
+// doubleHasher, linearProber, powerOfTwoHasher or XORPowerOfTwoHasher; Hasher
+// murmurHasher; Bucket_Size 4/8/16/32 on the primary level; at most one
+// recursive (backing) table.
+#pragma once
+#include <cooperative_groups.h>
+#include <stdexcept>
+#include <cstdint>
+#include <cstddef>
+#include "poggers_b200.h"
+#include "poggers_b200/level.cuh"
+
+namespace poggers_b200 {
+
+namespace hashers {
+template <typename Key, std::size_t Partition_size = 1>
+struct murmurHasher {};
+}  // namespace hashers
+
+namespace representations {
+template <typename Key, typename Val>
+struct key_val_pair {};
+template <typename Key, typename Val>
+struct key_container {};
+template <template <typename, typename> class Container, typename SmallKey>
+struct dynamic_container {
+    template <typename Key, typename Val>
+    struct representation {};
+};
+}  // namespace representations
+
+namespace probing_schemes {
+template <typename Key, std::size_t P, template <typename, std::size_t> class H, std::size_t M>
+struct doubleHasher {};
+template <typename Key, std::size_t P, template <typename, std::size_t> class H, std::size_t M>
+struct linearProber {};
+template <typename Key, std::size_t P, template <typename, std::size_t> class H, std::size_t M>
+struct powerOfTwoHasher {};
+template <typename Key, std::size_t P, template <typename, std::size_t> class H, std::size_t M>
+struct XORPowerOfTwoHasher {};
+}  // namespace probing_schemes
+
+namespace insert_schemes {
+#define PG_SCHEME_PARAMS                                                                                       \
+    typename Key, typename Val, std::size_t P, std::size_t B, template <typename, typename> class Rep, std::size_t M, \
+        template <typename, std::size_t> class H,                                                              \
+        template <typename, std::size_t, template <typename, std::size_t> class, std::size_t> class Probe
+template <PG_SCHEME_PARAMS>
+struct bucket_insert {};
+template <PG_SCHEME_PARAMS>
+struct power_of_n_insert_shortcut_scheme {};
+#undef PG_SCHEME_PARAMS
+}  // namespace insert_schemes
+
+namespace sizing {
+// size_in_num_slots<N>: one slot count per table level (default_sizing.cuh:30-95)
+template <std::size_t Num_Tables>
+struct size_in_num_slots {
+    uint64_t slots[Num_Tables];
+    uint64_t i = 0;
+    template <class... T>
+    explicit size_in_num_slots(T... s) : slots{(uint64_t)s...}
+    {
+        static_assert(sizeof...(T) == Num_Tables, "one slot count per level");
+    }
+    uint64_t next() { return ++i <= Num_Tables ? slots[i - 1] : end(); }
+    void reset() { i = 0; }
+    uint64_t end() const { return ~uint64_t(0); }
+    uint64_t total() const
+    {
+        uint64_t t = 0;
+        for (std::size_t j = 0; j < Num_Tables; j++) t += slots[j];
+        return t;
+    }
+};
+}  // namespace sizing
+
+namespace detail {
+template <template <typename, typename> class Rep, typename Val>
+struct format_of;
+template <>
+struct format_of<representations::key_val_pair, uint64_t> { static constexpr uint32_t value = PG_FMT_KV64; };
+template <template <typename, typename> class C, typename S>
+struct is_dyn {};
+
+template <template <typename, typename> class Rep>
+struct rep_kind { static constexpr int value = -1; };
+template <>
+struct rep_kind<representations::key_val_pair> { static constexpr int value = 0; };
+template <>
+struct rep_kind<representations::dynamic_container<representations::key_val_pair, uint16_t>::template representation> {
+    static constexpr int value = 1;
+};
+template <>
+struct rep_kind<representations::dynamic_container<representations::key_container, uint16_t>::template representation> {
+    static constexpr int value = 2;
+};
+
+template <template <typename, typename, std::size_t, std::size_t, template <typename, typename> class, std::size_t,
+                    template <typename, std::size_t> class,
+                    template <typename, std::size_t, template <typename, std::size_t> class, std::size_t> class>
+          class S>
+struct scheme_id { static constexpr int value = -1; };
+template <>
+struct scheme_id<insert_schemes::bucket_insert> { static constexpr int value = PG_SCHEME_BUCKET; };
+template <>
+struct scheme_id<insert_schemes::power_of_n_insert_shortcut_scheme> { static constexpr int value = PG_SCHEME_TWO_CHOICE; };
+
+template <template <typename, std::size_t, template <typename, std::size_t> class, std::size_t> class Pr>
+struct probe_id { static constexpr int value = -1; };
+template <>
+struct probe_id<probing_schemes::doubleHasher> { static constexpr int value = PG_PROBE_DOUBLE; };
+template <>
+struct probe_id<probing_schemes::linearProber> { static constexpr int value = PG_PROBE_LINEAR; };
+template <>
+struct probe_id<probing_schemes::powerOfTwoHasher> { static constexpr int value = PG_PROBE_P2; };
+template <>
+struct probe_id<probing_schemes::XORPowerOfTwoHasher> { static constexpr int value = PG_PROBE_XOR_P2; };
+}  // namespace detail
+
+namespace tables {
+
+// terminal of the recursion, like recursive_end_table (tables/recursive_end_table.cuh)
+struct recursive_end_table {
+    static constexpr bool kIsTable = false;
+};
+
+template <typename Key, typename Val, template <typename, typename> class Internal_Rep, std::size_t Partition_Size,
+          std::size_t Bucket_Size,
+          template <typename, typename, std::size_t, std::size_t, template <typename, typename> class, std::size_t,
+                    template <typename, std::size_t> class,
+                    template <typename, std::size_t, template <typename, std::size_t> class, std::size_t> class>
+          class Insert_Scheme,
+          std::size_t Max_Probes,
+          template <typename, std::size_t, template <typename, std::size_t> class, std::size_t> class Probing_Scheme,
+          template <typename, std::size_t> class Hasher, bool Is_Recursive = false,
+          typename Recursive_Type = recursive_end_table>
+struct static_table {
+    static constexpr bool kIsTable = true;
+    using key_type = Key;
+    using val_type = Val;
+    using my_type = static_table;
+    static constexpr int kFmt = detail::rep_kind<Internal_Rep>::value;
+    static constexpr int kScheme = detail::scheme_id<Insert_Scheme>::value;
+    static constexpr int kProbe = detail::probe_id<Probing_Scheme>::value;
+    static constexpr int G = (int)Partition_Size;
+    static constexpr int B = (int)Bucket_Size;
+    static_assert(std::is_same<Key, uint64_t>::value, "keys are uint64_t");
+    static_assert(kFmt >= 0, "representation not supported on this path");
+    static_assert(kFmt != 0 || std::is_same<Val, uint64_t>::value, "key_val_pair tables map uint64_t -> uint64_t");
+    static_assert(kFmt == 0 || std::is_same<Val, uint16_t>::value, "filters carry uint16_t values");
+    static_assert(kScheme >= 0 && kProbe >= 0, "insert / probing scheme not supported on this path");
+    static_assert(B == 4 || B == 8 || B == 16 || B == 32, "primary bucket size 4, 8, 16 or 32");
+    static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "tile of 1..16 lanes");
+    using ops = pg::table_ops<kFmt, B, G, kScheme, Is_Recursive>;
+    using dev_val = typename pg::fmt_t<kFmt>::V;
+
+    pg::table_desc desc;
+    pg_table *handle;
+
+    static void fill_level(pg_level_config &L, uint64_t nslots)
+    {
+        L.nslots = nslots;
+        L.bucket_size = (uint32_t)Bucket_Size;
+        L.max_probes = (uint32_t)Max_Probes;
+        L.scheme = (uint32_t)kScheme;
+        L.probe = (uint32_t)kProbe;
+    }
+
+    template <typename Sizing_Type>
+    static pg_table_config config_from(Sizing_Type *sizing)
+    {
+        pg_table_config c{};
+        c.format = (uint32_t)kFmt;
+        c.tile = (uint32_t)Partition_Size;
+        c.nlevels = Is_Recursive ? 2 : 1;
+        uint64_t n0 = sizing->next();
+        if (n0 == sizing->end())
+            throw std::runtime_error("Hash Table expects a num_slots from the sizing, but the size container is empty\n");
+        fill_level(c.levels[0], n0);
+        if constexpr (Is_Recursive) {
+            static_assert(Recursive_Type::kIsTable, "recursive table type");
+            uint64_t n1 = sizing->next();
+            if (n1 == sizing->end())
+                throw std::runtime_error("Hash Table expects a num_slots from the sizing, but the size container is empty\n");
+            Recursive_Type::fill_level(c.levels[1], n1);
+            c.levels[1].scheme = (uint32_t)Recursive_Type::kScheme;
+            c.levels[1].probe = (uint32_t)Recursive_Type::kProbe;
+        }
+        if (sizing->next() != sizing->end())
+            throw std::runtime_error("Hash Table Does not expect recursion but the size container is not empty.\n");
+        return c;
+    }
+
+    // static_table::generate_on_device (base_table.cuh:110-145): returns a device pointer
+    template <typename Sizing_Type>
+    __host__ static my_type *generate_on_device(Sizing_Type *sizing, uint64_t seed)
+    {
+        pg_table_config c = config_from(sizing);
+        pg_table *h = nullptr;
+        pg_status st = pg_table_create(&c, seed, &h);
+        if (st != PG_OK) throw std::runtime_error(pg_status_string(st));
+        my_type host;
+        host.handle = h;
+        pg_level_info info;
+        // the descriptor the bulk kernels use, rebuilt here for device callers
+        for (uint32_t l = 0; l < c.nlevels; l++) {
+            pg_table_level_info(h, l, &info);
+            pg::level_desc &D = host.desc.lv[l];
+            const pg_level_config &L = c.levels[l];
+            const uint32_t kb = kFmt == 0 ? 8u : 2u, vb = kFmt == 0 ? 8u : (kFmt == 1 ? 2u : 0u);
+            D.base = (unsigned char *)info.d_buckets;
+            D.nbmod = pg::make_fastmod64(info.nbuckets);
+            D.seed = info.seed;
+            D.seed2 = info.seed * info.seed;
+            D.bucket_size = L.bucket_size;
+            D.max_probes = L.max_probes;
+            D.scheme = L.scheme;
+            D.probe = L.probe;
+            D.bucket_bytes = L.bucket_size * (kb + vb);
+            D.val_offset = L.bucket_size * kb;
+        }
+        host.desc.nlevels = c.nlevels;
+        host.desc.format = (uint32_t)kFmt;
+        my_type *dev = nullptr;
+        if (cudaMalloc(&dev, sizeof(my_type)) != cudaSuccess) {
+            pg_table_destroy(h);
+            throw std::runtime_error("cudaMalloc of the table descriptor failed");
+        }
+        cudaMemcpy(dev, &host, sizeof(my_type), cudaMemcpyHostToDevice);
+        return dev;
+    }
+
+    __host__ static void free_on_device(my_type *dev)
+    {
+        my_type host;
+        cudaMemcpy(&host, dev, sizeof(my_type), cudaMemcpyDeviceToHost);
+        pg_table_destroy(host.handle);
+        cudaFree(dev);
+    }
+
+    // the C-ABI handle behind a device pointer (to call the bulk entry points)
+    __host__ static pg_table *host_handle(my_type *dev)
+    {
+        my_type host;
+        cudaMemcpy(&host, dev, sizeof(my_type), cudaMemcpyDeviceToHost);
+        return host.handle;
+    }
+
+    __device__ __forceinline__ pg::group<G> group_of(const cooperative_groups::thread_block_tile<Partition_Size> &) const
+    {
+        return pg::group<G>::make();
+    }
+
+    __device__ bool insert(cooperative_groups::thread_block_tile<Partition_Size> tile, Key key, Val val)
+    {
+        return ops::insert(desc, group_of(tile), key, (dev_val)val);
+    }
+    __device__ bool insert(cooperative_groups::thread_block_tile<Partition_Size> tile, Key key)
+    {
+        return insert(tile, key, Val(0));
+    }
+    __device__ bool query(cooperative_groups::thread_block_tile<Partition_Size> tile, Key key, Val &val)
+    {
+        dev_val v = 0;
+        bool r = ops::query(desc, group_of(tile), key, v);
+        if (r) val = (Val)v;
+        return r;
+    }
+    __device__ bool remove(cooperative_groups::thread_block_tile<Partition_Size> tile, Key key)
+    {
+        return ops::remove(desc, group_of(tile), key);
+    }
+
+    __device__ __inline__ cooperative_groups::thread_block_tile<Partition_Size> get_my_tile()
+    {
+        return cooperative_groups::tiled_partition<Partition_Size>(cooperative_groups::this_thread_block());
+    }
+    __host__ static uint64_t get_block_size(uint64_t) { return 1024; }
+    __host__ static uint64_t get_num_blocks(uint64_t n) { return (Partition_Size * n - 1) / get_block_size(n) + 1; }
+    __host__ uint64_t host_bytes_in_use() { return pg_table_bytes(host_handle(this)); }
+};
+
+}  // namespace tables
+
+namespace data_structs {
+using tiny_static_table_4 =
+    tables::static_table<uint64_t, uint16_t,
+                         representations::dynamic_container<representations::key_val_pair, uint16_t>::representation, 4,
+                         4, insert_schemes::bucket_insert, 20, probing_schemes::doubleHasher, hashers::murmurHasher>;
+using tcf = tables::static_table<uint64_t, uint16_t,
+                                 representations::dynamic_container<representations::key_val_pair, uint16_t>::representation,
+                                 4, 16, insert_schemes::power_of_n_insert_shortcut_scheme, 2,
+                                 probing_schemes::doubleHasher, hashers::murmurHasher, true, tiny_static_table_4>;
+using hash_table_64 = tables::static_table<uint64_t, uint64_t, representations::key_val_pair, 4, 16,
+                                           insert_schemes::bucket_insert, 20, probing_schemes::doubleHasher,
+                                           hashers::murmurHasher>;
+}  // namespace data_structs
+
+}  // namespace poggers_b200

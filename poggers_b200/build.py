@@ -74,5 +74,28 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     return LIB
 
 
+TEST_SRC = ROOT / "tests" / "cpp"
+TEST_BIN = TEST_SRC / "_bin"
+
+
+def build_tests(verbose: bool = False) -> list[Path]:
+    """C++ drivers written against the reference-shaped template API (tests/cpp)."""
+    lib = build()
+    TEST_BIN.mkdir(exist_ok=True)
+    out = []
+    for src in sorted(TEST_SRC.glob("*.cu")):
+        exe = TEST_BIN / src.stem
+        if _needs(exe, [src, lib] + _headers()):
+            cmd = [nvcc(), *NVCC_FLAGS, str(src), "-o", str(exe), f"-L{PKG}", "-lpoggers_b200",
+                   f"-Xlinker", f"-rpath={PKG}", "-Xlinker", "-rpath=$ORIGIN/../../../poggers_b200"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {src.name}:\n{r.stdout}\n{r.stderr}")
+        out.append(exe)
+        if verbose:
+            print(f"built {exe}")
+    return out
+
+
 if __name__ == "__main__":
     build(verbose=True, extra=sys.argv[1:])
