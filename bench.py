@@ -35,7 +35,11 @@ sys.path.insert(0, str(ROOT))
 
 NSLOTS = 1 << 26
 BUCKET = 8
-TILE = 4
+TILE = 4          # the reference's Partition_Size for this table (semantics)
+LANES = 2         # lanes per key the kernels use (launch shape; results do not depend on it)
+SPLIT = True      # keys then values inside each bucket
+BLOCK_THREADS = 256
+BLOCKS_PER_SM = 32
 PROBES = 20
 LOAD = 0.9
 SEED = 43
@@ -138,7 +142,10 @@ def run_ours(args, rank, world):
     ok = torch.empty(n, dtype=torch.uint8, device=dev)
     found = torch.empty(nq, dtype=torch.uint8, device=dev)
     qv = torch.empty(nq, dtype=torch.int64, device=dev)
-    table = pg.Table(pg.data_structs.hash_table_64(NSLOTS, tile=TILE, bucket=BUCKET, max_probes=PROBES), SEED)
+    cfg = pg.data_structs.hash_table_64(NSLOTS, tile=TILE, bucket=BUCKET, max_probes=PROBES)
+    cfg.split = SPLIT
+    table = pg.Table(cfg, SEED)
+    table.set_launch(BLOCK_THREADS, BLOCKS_PER_SM, 0, LANES)
     stream = torch.cuda.current_stream()
 
     def step(ev=None):
@@ -210,6 +217,8 @@ def run_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 keys)",
         "config": {"workload": WORKLOAD, "slots": NSLOTS, "inserts": n, "queries": nq,
+                   "launch": {"lanes_per_key": LANES, "block_threads": BLOCK_THREADS,
+                              "blocks_per_sm": BLOCKS_PER_SM, "bucket_layout": "split" if SPLIT else "interleaved"},
                    "parallelism": f"independent table per GPU x{world}",
                    "l2": "inputs larger than L2 (1 GiB table, 126 MB L2)"},
         "roofline": {"bound": "hbm", "kernel": f"bulk_{dom}", "achieved": round(achieved, 1),

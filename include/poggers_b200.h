@@ -86,11 +86,24 @@ typedef struct pg_level_config {
     uint32_t probe;       /* PG_PROBE_* */
 } pg_level_config;
 
+/* table flags */
+enum {
+    /* Keep each bucket's keys contiguous, then its values ([B keys | B vals]),
+     * instead of the reference's {key, val} slots.  Same results; see the
+     * layout notes in DESIGN.md. */
+    PG_TABLE_SPLIT_BUCKETS = 1u,
+    /* uint64 tables (PG_FMT_KV64, bucket_insert primary, reference layout):
+     * keep one fingerprint byte per slot in a separate array (1/16 of the
+     * slot bytes) that the kernels hold in L2, so probes touch DRAM only for
+     * slots whose fingerprint matches.  Same results. */
+    PG_TABLE_FINGERPRINTS = 2u
+};
+
 typedef struct pg_table_config {
     uint32_t format;   /* PG_FMT_* */
     uint32_t tile;     /* lanes per key (the reference's Partition_Size): 1,2,4,8,16; <= level-0 bucket size */
     uint32_t nlevels;  /* 1, or 2 = primary + backing (static_table's recursive table) */
-    uint32_t reserved; /* must be 0 */
+    uint32_t flags;    /* PG_TABLE_* bits, 0 = the reference's slot layout */
     pg_level_config levels[2];
 } pg_table_config;
 
@@ -118,11 +131,16 @@ pg_status pg_table_level_info(const pg_table *t, uint32_t level, pg_level_info *
 /* Device bytes owned by the table (host_bytes_in_use). */
 uint64_t pg_table_bytes(const pg_table *t);
 
-/* Launch shape: threads per block (multiple of the tile, <= 1024) and a cap on
- * blocks (0 = enough blocks for one key per group, capped at blocks_per_sm
- * resident blocks on every SM).  block_threads == tile with max_blocks == 1
- * runs the batch strictly in order on one group (deterministic layout). */
-pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks);
+/* Launch shape of the bulk kernels: threads per block (<= 256, a multiple of
+ * the lanes per key; 0 = 256), blocks per SM (0 = 32), a cap on blocks (0 =
+ * none) and the lanes that serve one key (0 = the config's tile; 1, 2, 4, 8
+ * or 16, at most the level-0 bucket size).  The lanes per key never change a
+ * result: filled slots always form a prefix of each bucket, so the
+ * reference's tile-wide stripes decide exactly what a whole-bucket scan
+ * decides.  block_threads == lanes with max_blocks == 1 runs the batch
+ * strictly in order on one group (the reference's serial layout). */
+pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
+                              uint32_t lanes_per_key);
 
 /* Bulk insert of n keys (and values; d_vals may be NULL = all 0).
  * d_ok[i] (optional) = 1 if key i was placed; d_fail_count (optional) += failures. */
@@ -149,6 +167,61 @@ pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_s
  * Synchronous. */
 pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst, uint64_t bytes);
 pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes);
+
+/* ---------------------------------------------------------------------------
+ * Slab allocator: fixed-size objects from slabs of 4096.
+ *
+ * Replaces one_size_slab_allocator<N> (allocators/slab_one_size.cuh:58-659):
+ *   pg_slab_create        <- generate_on_device(num_allocs, size)     slab_one_size.cuh:84-140
+ *   pg_slab_destroy       <- free_on_device                            slab_one_size.cuh:142-180
+ *   pg_slab_bulk_malloc   <- malloc() one thread per allocation        slab_one_size.cuh:186-288
+ *                            (driver: tests/src/slab_one_size_tests.cu:72-104)
+ *   pg_slab_bulk_free     <- free(void*)                               slab_one_size.cuh:428-463
+ *   pg_slab_report        <- report_fill / report_max                  slab_one_size.cuh:628-654
+ * Capacity is ceil(num_allocs / 4096) * 4096 objects.  A malloc that finds no
+ * object after 25 bounded attempts returns NULL, like the reference.
+ * --------------------------------------------------------------------------- */
+typedef struct pg_slab pg_slab;
+typedef struct pg_slab_set pg_slab_set;
+
+#define PG_SLAB_MAX_CLASSES 16
+
+typedef struct pg_slab_info_t {
+    void *pool;               /* device address of object 0 */
+    uint64_t pool_bytes;
+    uint64_t object_bytes;
+    uint64_t capacity;        /* objects */
+    uint64_t nslabs;
+    uint64_t *d_stats;        /* device: [0] double frees, [1] frees of foreign / misaligned pointers */
+} pg_slab_info_t;
+
+pg_status pg_slab_create(uint64_t num_allocs, uint64_t object_bytes, pg_slab **out);
+pg_status pg_slab_destroy(pg_slab *a);
+/* Mark every object free again (stream-ordered). */
+pg_status pg_slab_reset(pg_slab *a, pg_stream_t stream);
+pg_status pg_slab_info(const pg_slab *a, pg_slab_info_t *out);
+/* d_ptrs[i] = a distinct object or NULL; d_fail_count (optional) += NULLs. */
+pg_status pg_slab_bulk_malloc(pg_slab *a, uint64_t n, void **d_ptrs, uint64_t *d_fail_count, pg_stream_t stream);
+/* Free d_ptrs[0..n) (NULL entries are skipped); d_bad_count (optional) +=
+ * double frees and pointers that are not objects of this pool. */
+pg_status pg_slab_bulk_free(pg_slab *a, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count, pg_stream_t stream);
+/* d_out[0] += free objects, d_out[1] += fully free slabs. */
+pg_status pg_slab_count_free(pg_slab *a, uint64_t *d_out, pg_stream_t stream);
+/* Synchronous report: free slabs (report_fill), slabs (report_max), free objects, double frees. */
+pg_status pg_slab_report(pg_slab *a, uint64_t *free_slabs, uint64_t *max_slabs, uint64_t *free_objects,
+                         uint64_t *double_frees);
+
+/* Size classes: one pool per class (class_bytes strictly increasing, at most
+ * PG_SLAB_MAX_CLASSES).  A request of s bytes is served by the smallest class
+ * with class_bytes >= s; larger requests get NULL. */
+pg_status pg_slab_set_create(uint32_t nclasses, const uint64_t *class_bytes, const uint64_t *num_allocs,
+                             pg_slab_set **out);
+pg_status pg_slab_set_destroy(pg_slab_set *s);
+pg_slab *pg_slab_set_class(pg_slab_set *s, uint32_t c);
+pg_status pg_slab_set_bulk_malloc(pg_slab_set *s, const uint32_t *d_sizes, uint64_t n, void **d_ptrs,
+                                  uint64_t *d_fail_count, pg_stream_t stream);
+pg_status pg_slab_set_bulk_free(pg_slab_set *s, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count,
+                                pg_stream_t stream);
 
 /* Host-side helpers used by tests (no GPU needed). */
 uint64_t pg_host_murmur64a(uint64_t key, uint64_t seed);

@@ -236,7 +236,6 @@ struct static_table {
             D.scheme = L.scheme;
             D.probe = L.probe;
             D.bucket_bytes = L.bucket_size * (kb + vb);
-            D.val_offset = L.bucket_size * kb;
         }
         host.desc.nlevels = c.nlevels;
         host.desc.format = (uint32_t)kFmt;

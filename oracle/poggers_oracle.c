@@ -718,3 +718,71 @@ void pgo_splitmix64_fill(uint64_t seed, uint64_t start, uint64_t n, uint64_t *ou
         out[i] = z ^ (z >> 31);
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Slab allocator model (one_size_slab_allocator, allocators/slab_one_size.cuh):
+ * a pool of ceil(num_allocs / 4096) * 4096 objects; malloc returns a free
+ * object or fails when none is left; free returns an object, and a free of an
+ * object that is already free is a double free (offset_slab.cuh:473-478).
+ * Sequential and deterministic (lowest free offset first): object identities
+ * differ from a concurrent allocator's, but every count must agree. */
+struct pgo_slab {
+    uint64_t capacity;
+    uint64_t nfree;
+    uint64_t *bits; /* 1 = free */
+};
+
+pgo_slab *pgo_slab_create(uint64_t num_allocs)
+{
+    if (num_allocs == 0) return NULL;
+    pgo_slab *s = (pgo_slab *)calloc(1, sizeof(pgo_slab));
+    s->capacity = ((num_allocs - 1) / 4096 + 1) * 4096;
+    s->nfree = s->capacity;
+    s->bits = (uint64_t *)malloc(s->capacity / 8);
+    memset(s->bits, 0xFF, s->capacity / 8);
+    return s;
+}
+
+void pgo_slab_destroy(pgo_slab *s)
+{
+    if (!s) return;
+    free(s->bits);
+    free(s);
+}
+
+uint64_t pgo_slab_capacity(const pgo_slab *s) { return s->capacity; }
+uint64_t pgo_slab_free_objects(const pgo_slab *s) { return s->nfree; }
+
+/* offsets[i] = object offset or ~0; returns failures */
+uint64_t pgo_slab_malloc(pgo_slab *s, uint64_t n, uint64_t *offsets)
+{
+    uint64_t fails = 0, w = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        while (w < s->capacity / 64 && s->bits[w] == 0) w++;
+        if (w == s->capacity / 64) {
+            offsets[i] = ~(uint64_t)0;
+            fails++;
+            continue;
+        }
+        int b = __builtin_ctzll(s->bits[w]);
+        s->bits[w] &= s->bits[w] - 1;
+        s->nfree--;
+        offsets[i] = w * 64 + (uint64_t)b;
+    }
+    return fails;
+}
+
+/* returns the number of rejected frees (double frees, offsets out of range) */
+uint64_t pgo_slab_free(pgo_slab *s, uint64_t n, const uint64_t *offsets)
+{
+    uint64_t bad = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t o = offsets[i];
+        if (o >= s->capacity) { bad++; continue; }
+        uint64_t m = 1ULL << (o % 64);
+        if (s->bits[o / 64] & m) { bad++; continue; }
+        s->bits[o / 64] |= m;
+        s->nfree++;
+    }
+    return bad;
+}

@@ -12,7 +12,7 @@
  * byte-for-byte with a dump of the reference's own device table.
  *
  * Parity pin: murmur and probe sequences are pinned against the reference's
- * own __host__ code compiled from its headers (oracle/ref_pin.cpp), and the
+ * own __host__ code compiled from its headers (oracle/ref_host_pin.cpp), and the
  * sequential table layout is pinned against golden dumps produced by the
  * reference's CUDA build (tests/golden/, generated by
  * tests/golden/make_golden.py).
@@ -105,6 +105,15 @@ uint64_t pgo_mt_bulk_insert(pgo_table *t, const uint64_t *keys, const uint64_t *
 uint64_t pgo_mt_bulk_query(pgo_table *t, const uint64_t *keys, uint64_t n, uint64_t *vals, uint8_t *found, int nthreads);
 uint64_t pgo_mt_bulk_remove(pgo_table *t, const uint64_t *keys, uint64_t n, uint8_t *ok, int nthreads);
 int pgo_online_cores(void);
+
+/* slab allocator model: counts of a fixed-size object pool */
+typedef struct pgo_slab pgo_slab;
+pgo_slab *pgo_slab_create(uint64_t num_allocs);
+void pgo_slab_destroy(pgo_slab *s);
+uint64_t pgo_slab_capacity(const pgo_slab *s);
+uint64_t pgo_slab_free_objects(const pgo_slab *s);
+uint64_t pgo_slab_malloc(pgo_slab *s, uint64_t n, uint64_t *offsets);
+uint64_t pgo_slab_free(pgo_slab *s, uint64_t n, const uint64_t *offsets);
 
 /* splitmix64 key stream: key i = mix(seed + (i+1) * 0x9E3779B97F4A7C15) */
 void pgo_splitmix64_fill(uint64_t seed, uint64_t start, uint64_t n, uint64_t *out);

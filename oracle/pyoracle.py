@@ -89,6 +89,16 @@ def lib():
         L.pgo_mt_bulk_remove.argtypes = [C.c_void_p, U64P, C.c_uint64, U8P, C.c_int]
         L.pgo_online_cores.restype = C.c_int
         L.pgo_splitmix64_fill.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, U64P]
+        L.pgo_slab_create.restype = C.c_void_p
+        L.pgo_slab_create.argtypes = [C.c_uint64]
+        L.pgo_slab_destroy.argtypes = [C.c_void_p]
+        for f in ("pgo_slab_capacity", "pgo_slab_free_objects"):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_void_p]
+        L.pgo_slab_malloc.restype = C.c_uint64
+        L.pgo_slab_malloc.argtypes = [C.c_void_p, C.c_uint64, U64P]
+        L.pgo_slab_free.restype = C.c_uint64
+        L.pgo_slab_free.argtypes = [C.c_void_p, C.c_uint64, U64P]
         _lib = L
     return _lib
 
@@ -205,3 +215,32 @@ class OracleTable:
 
 def online_cores() -> int:
     return lib().pgo_online_cores()
+
+
+class OracleSlab:
+    """Sequential model of one fixed-size object pool (counts only)."""
+
+    def __init__(self, num_allocs: int):
+        self.h = lib().pgo_slab_create(num_allocs)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pgo_slab_destroy(self.h)
+            self.h = None
+
+    @property
+    def capacity(self) -> int:
+        return lib().pgo_slab_capacity(self.h)
+
+    @property
+    def free_objects(self) -> int:
+        return lib().pgo_slab_free_objects(self.h)
+
+    def malloc(self, n: int):
+        out = np.zeros(n, dtype=np.uint64)
+        fails = lib().pgo_slab_malloc(self.h, n, _p64(out))
+        return out, fails
+
+    def free(self, offsets) -> int:
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        return lib().pgo_slab_free(self.h, len(offsets), _p64(offsets))

@@ -20,14 +20,19 @@ to a CPU path: a missing or unloadable library raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libpoggers_b200.so"
+# POGGERS_B200_LIB selects another build of the same library (e.g. a variant
+# compiled with different launch bounds, for a side-by-side measurement)
+LIB_PATH = Path(os.environ.get("POGGERS_B200_LIB", str(_PKG / "libpoggers_b200.so")))
 
 # ---- enums (include/poggers_b200.h)
 PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT = range(7)
+PG_TABLE_SPLIT_BUCKETS = 1
+PG_TABLE_FINGERPRINTS = 2
 FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
 SCHEME_BUCKET, SCHEME_TWO_CHOICE = 0, 1
 PROBE_DOUBLE, PROBE_LINEAR, PROBE_P2, PROBE_XOR_P2 = 0, 1, 2, 3
@@ -49,12 +54,17 @@ class _LevelConfig(C.Structure):
 
 class _TableConfig(C.Structure):
     _fields_ = [("format", C.c_uint32), ("tile", C.c_uint32), ("nlevels", C.c_uint32),
-                ("reserved", C.c_uint32), ("levels", _LevelConfig * 2)]
+                ("flags", C.c_uint32), ("levels", _LevelConfig * 2)]
 
 
 class _LevelInfo(C.Structure):
     _fields_ = [("nbuckets", C.c_uint64), ("nslots", C.c_uint64), ("bytes", C.c_uint64),
                 ("seed", C.c_uint64), ("d_buckets", C.c_void_p)]
+
+
+class _SlabInfo(C.Structure):
+    _fields_ = [("pool", C.c_void_p), ("pool_bytes", C.c_uint64), ("object_bytes", C.c_uint64),
+                ("capacity", C.c_uint64), ("nslabs", C.c_uint64), ("d_stats", C.c_void_p)]
 
 
 _lib = None
@@ -64,6 +74,9 @@ EXPORTED = (
     "pg_table_level_info", "pg_table_bytes", "pg_table_set_launch", "pg_bulk_insert", "pg_bulk_query",
     "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
+    "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
+    "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
+    "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
 )
 
 
@@ -90,7 +103,7 @@ def lib() -> C.CDLL:
     L.pg_table_bytes.restype = U64
     L.pg_table_bytes.argtypes = [V]
     L.pg_table_set_launch.restype = C.c_int
-    L.pg_table_set_launch.argtypes = [V, U32, U32, U32]
+    L.pg_table_set_launch.argtypes = [V, U32, U32, U32, U32]
     L.pg_bulk_insert.restype = C.c_int
     L.pg_bulk_insert.argtypes = [V, P, P, U64, P, P, P]
     L.pg_bulk_query.restype = C.c_int
@@ -103,6 +116,32 @@ def lib() -> C.CDLL:
     L.pg_table_dump_level.argtypes = [V, U32, P, U64]
     L.pg_table_load_level.restype = C.c_int
     L.pg_table_load_level.argtypes = [V, U32, P, U64]
+    L.pg_slab_create.restype = C.c_int
+    L.pg_slab_create.argtypes = [U64, U64, C.POINTER(V)]
+    L.pg_slab_destroy.restype = C.c_int
+    L.pg_slab_destroy.argtypes = [V]
+    L.pg_slab_reset.restype = C.c_int
+    L.pg_slab_reset.argtypes = [V, P]
+    L.pg_slab_info.restype = C.c_int
+    L.pg_slab_info.argtypes = [V, C.POINTER(_SlabInfo)]
+    L.pg_slab_bulk_malloc.restype = C.c_int
+    L.pg_slab_bulk_malloc.argtypes = [V, U64, P, P, P]
+    L.pg_slab_bulk_free.restype = C.c_int
+    L.pg_slab_bulk_free.argtypes = [V, P, U64, P, P]
+    L.pg_slab_count_free.restype = C.c_int
+    L.pg_slab_count_free.argtypes = [V, P, P]
+    L.pg_slab_report.restype = C.c_int
+    L.pg_slab_report.argtypes = [V, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]
+    L.pg_slab_set_create.restype = C.c_int
+    L.pg_slab_set_create.argtypes = [U32, C.POINTER(U64), C.POINTER(U64), C.POINTER(V)]
+    L.pg_slab_set_destroy.restype = C.c_int
+    L.pg_slab_set_destroy.argtypes = [V]
+    L.pg_slab_set_class.restype = V
+    L.pg_slab_set_class.argtypes = [V, U32]
+    L.pg_slab_set_bulk_malloc.restype = C.c_int
+    L.pg_slab_set_bulk_malloc.argtypes = [V, P, U64, P, P, P]
+    L.pg_slab_set_bulk_free.restype = C.c_int
+    L.pg_slab_set_bulk_free.argtypes = [V, P, U64, P, P]
     L.pg_host_murmur64a.restype = U64
     L.pg_host_murmur64a.argtypes = [U64, U64]
     L.pg_host_fastmod.restype = U64
@@ -158,10 +197,13 @@ class TableConfig:
     format: int
     tile: int
     levels: list[Level] = field(default_factory=list)
+    split: bool = False  # PG_TABLE_SPLIT_BUCKETS: keys then values inside each bucket
+    fingerprints: bool = False  # PG_TABLE_FINGERPRINTS: L2-resident fingerprint byte per slot
 
     def c(self) -> _TableConfig:
         c = _TableConfig()
-        c.format, c.tile, c.nlevels, c.reserved = self.format, self.tile, len(self.levels), 0
+        c.format, c.tile, c.nlevels = self.format, self.tile, len(self.levels)
+        c.flags = (PG_TABLE_SPLIT_BUCKETS if self.split else 0) | (PG_TABLE_FINGERPRINTS if self.fingerprints else 0)
         for i, L in enumerate(self.levels):
             c.levels[i] = _LevelConfig(L.nslots, L.bucket_size, L.max_probes, L.scheme, L.probe)
         return c
@@ -171,7 +213,7 @@ class TableConfig:
             raise ValueError("sizing lists one slot count per level")
         return TableConfig(self.format, self.tile,
                            [Level(n, L.bucket_size, L.max_probes, L.scheme, L.probe)
-                            for n, L in zip(nslots, self.levels)])
+                            for n, L in zip(nslots, self.levels)], self.split, self.fingerprints)
 
 
 class sizing:
@@ -225,12 +267,15 @@ class Table:
     def clear(self, stream=None) -> None:
         _check(lib().pg_table_clear(self._h, _stream(stream)), "pg_table_clear")
 
-    def set_launch(self, block_threads: int = 0, blocks_per_sm: int = 0, max_blocks: int = 0) -> None:
-        _check(lib().pg_table_set_launch(self._h, block_threads, blocks_per_sm, max_blocks), "pg_table_set_launch")
+    def set_launch(self, block_threads: int = 0, blocks_per_sm: int = 0, max_blocks: int = 0,
+                   lanes_per_key: int = 0) -> None:
+        _check(lib().pg_table_set_launch(self._h, block_threads, blocks_per_sm, max_blocks, lanes_per_key),
+               "pg_table_set_launch")
 
-    def serial(self) -> None:
+    def serial(self, lanes_per_key: int = 0) -> None:
         """One group walks the batch in order (deterministic layout, for parity checks)."""
-        self.set_launch(self.config.tile, 1, 1)
+        lanes = 1 if self.config.fingerprints else (lanes_per_key or self.config.tile)
+        self.set_launch(lanes, 1, 1, lanes)
 
     def level_info(self, level: int) -> dict:
         info = _LevelInfo()
@@ -326,3 +371,110 @@ def host_probe_buckets(config: TableConfig, level: int, seed: int, key: int) -> 
     c = config.c()
     n = lib().pg_host_probe_buckets(C.byref(c), level, seed, key, out, 64)
     return list(out[:n])
+
+
+# ---------------------------------------------------------------- slab allocator
+class allocators:
+    """The reference's allocators/ (one_size_slab_allocator) on the slab kernels."""
+
+    class one_size_slab_allocator:
+        """Fixed-size objects from slabs of 4096 (allocators/slab_one_size.cuh:58-659)."""
+
+        def __init__(self, num_allocs: int, object_bytes: int):
+            h = C.c_void_p()
+            _check(lib().pg_slab_create(num_allocs, object_bytes, C.byref(h)), "pg_slab_create")
+            self._h = h
+            info = _SlabInfo()
+            _check(lib().pg_slab_info(h, C.byref(info)), "pg_slab_info")
+            self.pool = info.pool
+            self.pool_bytes = info.pool_bytes
+            self.object_bytes = info.object_bytes
+            self.capacity = info.capacity
+            self.nslabs = info.nslabs
+
+        @classmethod
+        def generate_on_device(cls, num_allocs: int, object_bytes: int):
+            return cls(num_allocs, object_bytes)
+
+        def free_on_device(self) -> None:
+            if getattr(self, "_h", None):
+                _check(lib().pg_slab_destroy(self._h), "pg_slab_destroy")
+                self._h = None
+
+        def __del__(self):
+            try:
+                self.free_on_device()
+            except Exception:
+                pass
+
+        @property
+        def handle(self):
+            return self._h
+
+        def reset(self, stream=None) -> None:
+            _check(lib().pg_slab_reset(self._h, _stream(stream)), "pg_slab_reset")
+
+        def bulk_malloc(self, ptrs_out, fail_count=None, stream=None, n: int | None = None) -> None:
+            """ptrs_out: int64 device tensor receiving one object address (or 0) per slot."""
+            n = ptrs_out.numel() if n is None else n
+            _check(lib().pg_slab_bulk_malloc(self._h, n, _ptr(ptrs_out), _ptr(fail_count), _stream(stream)),
+                   "pg_slab_bulk_malloc")
+
+        def bulk_free(self, ptrs, bad_count=None, stream=None, n: int | None = None) -> None:
+            n = ptrs.numel() if n is None else n
+            _check(lib().pg_slab_bulk_free(self._h, _ptr(ptrs), n, _ptr(bad_count), _stream(stream)),
+                   "pg_slab_bulk_free")
+
+        def report(self) -> dict:
+            fs, ms, fo, df = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+            _check(lib().pg_slab_report(self._h, C.byref(fs), C.byref(ms), C.byref(fo), C.byref(df)),
+                   "pg_slab_report")
+            return {"free_slabs": fs.value, "max_slabs": ms.value, "free_objects": fo.value,
+                    "double_frees": df.value}
+
+        def report_fill(self) -> int:
+            return self.report()["free_slabs"]
+
+        def report_max(self) -> int:
+            return self.report()["max_slabs"]
+
+    class size_class_set:
+        """One pool per size class; each request goes to the smallest class that fits."""
+
+        def __init__(self, class_bytes: list[int], num_allocs: list[int]):
+            n = len(class_bytes)
+            cb = (C.c_uint64 * n)(*class_bytes)
+            na = (C.c_uint64 * n)(*num_allocs)
+            h = C.c_void_p()
+            _check(lib().pg_slab_set_create(n, cb, na, C.byref(h)), "pg_slab_set_create")
+            self._h = h
+            self.class_bytes = list(class_bytes)
+
+        def free_on_device(self) -> None:
+            if getattr(self, "_h", None):
+                _check(lib().pg_slab_set_destroy(self._h), "pg_slab_set_destroy")
+                self._h = None
+
+        def __del__(self):
+            try:
+                self.free_on_device()
+            except Exception:
+                pass
+
+        def class_report(self, c: int) -> dict:
+            a = lib().pg_slab_set_class(self._h, c)
+            fs, ms, fo, df = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+            _check(lib().pg_slab_report(a, C.byref(fs), C.byref(ms), C.byref(fo), C.byref(df)), "pg_slab_report")
+            info = _SlabInfo()
+            _check(lib().pg_slab_info(a, C.byref(info)), "pg_slab_info")
+            return {"free_slabs": fs.value, "max_slabs": ms.value, "free_objects": fo.value, "double_frees": df.value,
+                    "pool": info.pool, "pool_bytes": info.pool_bytes, "capacity": info.capacity,
+                    "object_bytes": info.object_bytes}
+
+        def bulk_malloc(self, sizes, ptrs_out, fail_count=None, stream=None) -> None:
+            _check(lib().pg_slab_set_bulk_malloc(self._h, _ptr(sizes), sizes.numel(), _ptr(ptrs_out),
+                                                 _ptr(fail_count), _stream(stream)), "pg_slab_set_bulk_malloc")
+
+        def bulk_free(self, ptrs, bad_count=None, stream=None) -> None:
+            _check(lib().pg_slab_set_bulk_free(self._h, _ptr(ptrs), ptrs.numel(), _ptr(bad_count), _stream(stream)),
+                   "pg_slab_set_bulk_free")

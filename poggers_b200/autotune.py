@@ -1,0 +1,125 @@
+"""Launch-shape autotuner for the bulk kernels.
+
+The reference tunes its tile and bucket sizes by hand with separate test
+programs (tests/src/power_2_tests.cu:338-430, tests/src/test_cg_variations.cu:
+878-1040 sweep tile sizes 1-32 against bucket sizes 8-64).  Here the sweep is a
+library function: for one table shape it times bulk insert and bulk query on
+the device over
+
+  * lanes per key (the tile: 1, 2, 4, 8, 16; results do not depend on it,
+    because filled slots always form a prefix of each bucket),
+  * threads per block and resident blocks per SM,
+  * optionally the bucket size (which does change the table, and so is only
+    swept when the caller allows it),
+
+and returns the fastest shape.  Results are cached per GPU and table shape in
+a JSON file so a serving process pays for the sweep once.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import time
+from dataclasses import asdict, dataclass
+from pathlib import Path
+
+import numpy as np
+
+CACHE = Path(os.environ.get("POGGERS_B200_TUNE_CACHE", str(Path.home() / ".cache" / "poggers_b200_tune.json")))
+
+
+@dataclass
+class Shape:
+    tile: int
+    block_threads: int
+    blocks_per_sm: int
+    bucket: int
+    split: bool = False
+
+
+@dataclass
+class Result:
+    shape: Shape
+    insert_ms: float
+    query_ms: float
+
+    @property
+    def total_ms(self) -> float:
+        return self.insert_ms + self.query_ms
+
+
+def _dev(a: np.ndarray):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int16)).cuda()
+
+
+def time_shape(make_config, shape: Shape, seed: int, keys, vals, qkeys, reps: int = 3) -> Result:
+    """Median device time of one bulk insert (into a cleared table) and one bulk query."""
+    import torch
+    import poggers_b200 as pg
+
+    cfg = make_config(shape.tile, shape.bucket)
+    cfg.split = shape.split
+    t = pg.Table(cfg, seed)
+    t.set_launch(shape.block_threads, shape.blocks_per_sm, 0, shape.tile)
+    s = torch.cuda.current_stream()
+    ins, qry = [], []
+    for _ in range(reps + 1):
+        t.clear(s)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(s)
+        t.bulk_insert(keys, vals, None, None, s)
+        e1.record(s)
+        t.bulk_query(qkeys, None, None, None, s)
+        e2.record(s)
+        torch.cuda.synchronize()
+        ins.append(e0.elapsed_time(e1))
+        qry.append(e1.elapsed_time(e2))
+    t.free_on_device()
+    return Result(shape, float(np.median(ins[1:])), float(np.median(qry[1:])))
+
+
+def sweep(make_config, seed: int, keys, vals, qkeys, tiles=(1, 2, 4, 8), block_threads=(128, 256),
+          blocks_per_sm=(4, 8, 16), buckets=(None,), splits=(False,), reps: int = 3) -> list[Result]:
+    """Time every shape of the grid; `make_config(tile, bucket)` builds the table
+    configuration (bucket None = the table's own bucket size)."""
+    out = []
+    for tile, bt, bps, b, d in itertools.product(tiles, block_threads, blocks_per_sm, buckets, splits):
+        bucket = b if b is not None else make_config(1, None).levels[0].bucket_size
+        if tile > bucket or bt % tile:
+            continue
+        out.append(time_shape(make_config, Shape(tile, bt, bps, bucket, d), seed, keys, vals, qkeys, reps))
+    return out
+
+
+def best(results: list[Result]) -> Result:
+    return min(results, key=lambda r: r.total_ms)
+
+
+def cache_key(gpu_name: str, config) -> str:
+    L = config.levels[0]
+    return f"{gpu_name}|fmt{config.format}|b{L.bucket_size}|s{L.scheme}|p{L.probe}|n{L.nslots.bit_length()}|lv{len(config.levels)}"
+
+
+def tuned_shape(config, seed: int, keys, vals, qkeys, **grid) -> Shape:
+    """The cached best shape for this GPU and table shape, sweeping on a miss."""
+    import torch
+    name = torch.cuda.get_device_name()
+    key = cache_key(name, config)
+    cache = json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    if key in cache:
+        return Shape(**cache[key]["shape"])
+
+    def make(tile, bucket):
+        import poggers_b200 as pg
+        lv = [pg.Level(l.nslots, l.bucket_size if (i or bucket is None) else bucket, l.max_probes, l.scheme, l.probe)
+              for i, l in enumerate(config.levels)]
+        return pg.TableConfig(config.format, tile, lv)
+
+    res = sweep(make, seed, keys, vals, qkeys, **grid)
+    b = best(res)
+    cache[key] = {"shape": asdict(b.shape), "insert_ms": b.insert_ms, "query_ms": b.query_ms, "when": time.time()}
+    CACHE.parent.mkdir(parents=True, exist_ok=True)
+    CACHE.write_text(json.dumps(cache, indent=1))
+    return b.shape

@@ -57,21 +57,27 @@ def _compile(src: Path, extra: list[str]) -> Path:
     return obj
 
 
-def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
-    """Compile and link libpoggers_b200.so; returns its path."""
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, extra: list[str] | None = None, lib: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    """Compile and link libpoggers_b200.so (or a variant at `lib` built with
+    `extra` nvcc flags in `build_dir`); returns its path."""
+    global BUILD
+    lib = Path(lib) if lib else LIB
+    if build_dir:
+        BUILD = Path(build_dir)
+    BUILD.mkdir(parents=True, exist_ok=True)
     extra = list(extra or [])
     srcs = sorted(CSRC.glob("*.cu"))
     with cf.ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), srcs))
-    if _needs(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "shared", "-o", str(LIB), *map(str, objs)]
+    if _needs(lib, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "shared", "-o", str(lib), *map(str, objs)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     if verbose:
-        print(f"built {LIB}")
-    return LIB
+        print(f"built {lib}")
+    return lib
 
 
 TEST_SRC = ROOT / "tests" / "cpp"

@@ -31,8 +31,14 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
     if ((threadIdx.x & 31u) == (unsigned)(__ffs(am) - 1) && s) atomicAdd(count, (unsigned long long)s);
 }
 
+// Minimum resident 256-thread blocks per SM the register allocation must allow
+// (8 = full occupancy at 32 registers); a build-time knob measured by the tuner.
+#ifndef PG_MIN_BLOCKS
+#define PG_MIN_BLOCKS 1
+#endif
+
 template <int FMT, int B, int G, int S0, bool BK, int OP>
-__global__ void __launch_bounds__(256) k_bulk(table_desc t, bulk_args a)
+__global__ void __launch_bounds__(256, PG_MIN_BLOCKS) k_bulk(table_desc t, bulk_args a)
 {
     using F = fmt_t<FMT>;
     using V = typename F::V;
@@ -115,8 +121,8 @@ cudaError_t launch_b(int op, uint32_t tile, const table_desc &t, const bulk_args
 }
 
 template <int FMT>
-cudaError_t launch_fmt(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a, dim3 grid,
-                       dim3 block, cudaStream_t s)
+cudaError_t launch_fmt(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a,
+                       dim3 grid, dim3 block, cudaStream_t s)
 {
     switch (bucket) {
     case 4: return launch_b<FMT, 4>(op, tile, t, a, grid, block, s);
@@ -127,12 +133,15 @@ cudaError_t launch_fmt(int op, uint32_t bucket, uint32_t tile, const table_desc 
     }
 }
 
-// one per format, compiled in separate translation units
-cudaError_t launch_kv64(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a, dim3 grid,
-                        dim3 block, cudaStream_t s);
-cudaError_t launch_tagval16(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a,
-                            dim3 grid, dim3 block, cudaStream_t s);
-cudaError_t launch_tag16(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a, dim3 grid,
-                         dim3 block, cudaStream_t s);
+// one per internal format, compiled in separate translation units
+#define PG_DECLARE_LAUNCH(name)                                                                                   \
+    cudaError_t name(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a, dim3 grid, \
+                     dim3 block, cudaStream_t s)
+PG_DECLARE_LAUNCH(launch_kv64);
+PG_DECLARE_LAUNCH(launch_kv64_split);
+PG_DECLARE_LAUNCH(launch_tagval16);
+PG_DECLARE_LAUNCH(launch_tagval16_split);
+PG_DECLARE_LAUNCH(launch_tag16);
+PG_DECLARE_LAUNCH(launch_kv64_fp);
 
 }  // namespace pg

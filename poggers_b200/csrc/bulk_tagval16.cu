@@ -3,8 +3,7 @@
 
 namespace pg {
 
-cudaError_t launch_tagval16(int op, uint32_t bucket, uint32_t tile, const table_desc &t, const bulk_args &a, dim3 grid,
-                      dim3 block, cudaStream_t s)
+PG_DECLARE_LAUNCH(launch_tagval16)
 {
     return launch_fmt<FMT_TAGVAL16>(op, bucket, tile, t, a, grid, block, s);
 }

@@ -15,11 +15,15 @@ struct pg_table {
     table_desc desc;
     void *mem[2];
     uint64_t bytes[2];
+    void *fp;           // fingerprint bytes of level 0 (PG_TABLE_FINGERPRINTS)
+    uint64_t fp_bytes;
     int device;
     int num_sms;
     uint32_t block_threads;
     uint32_t blocks_per_sm;
     uint32_t max_blocks;
+    uint32_t lanes;  // lanes per key used by the kernels (defaults to the config's tile)
+    uint32_t ifmt;  // internal format: public format, split variant when PG_TABLE_SPLIT_BUCKETS
 };
 
 namespace {
@@ -27,9 +31,32 @@ namespace {
 uint32_t key_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : 2u; }
 uint32_t val_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : (fmt == PG_FMT_TAGVAL16 ? 2u : 0u); }
 
+bool split_layout(const pg_table_config *c)
+{
+    return (c->flags & PG_TABLE_SPLIT_BUCKETS) && c->format != PG_FMT_TAG16;
+}
+
+bool fingerprinted(const pg_table_config *c)
+{
+    return (c->flags & PG_TABLE_FINGERPRINTS) != 0;
+}
+
+uint32_t internal_format(const pg_table_config *c)
+{
+    if (fingerprinted(c)) return FMT_KV64_FP;
+    if (!split_layout(c)) return c->format;
+    return c->format == PG_FMT_KV64 ? (uint32_t)FMT_KV64_SPLIT : (uint32_t)FMT_TAGVAL16_SPLIT;
+}
+
 pg_status validate(const pg_table_config *c)
 {
-    if (!c || c->reserved != 0) return PG_ERR_INVALID;
+    if (!c || (c->flags & ~(uint32_t)(PG_TABLE_SPLIT_BUCKETS | PG_TABLE_FINGERPRINTS)) != 0) return PG_ERR_INVALID;
+    if (c->flags & PG_TABLE_FINGERPRINTS) {
+        // a fingerprint byte per uint64 slot, on a bucket_insert primary with the reference layout
+        if (c->format != PG_FMT_KV64 || (c->flags & PG_TABLE_SPLIT_BUCKETS) || c->nlevels < 1 ||
+            c->levels[0].scheme != PG_SCHEME_BUCKET)
+            return PG_ERR_UNSUPPORTED;
+    }
     if (c->format > PG_FMT_TAG16) return PG_ERR_INVALID;
     if (c->nlevels < 1 || c->nlevels > 2) return PG_ERR_INVALID;
     if (!(c->tile == 1 || c->tile == 2 || c->tile == 4 || c->tile == 8 || c->tile == 16)) return PG_ERR_INVALID;
@@ -56,10 +83,15 @@ pg_status cuda_status(cudaError_t e)
     return PG_ERR_CUDA;
 }
 
+uint32_t lanes_of(const pg_table *t)
+{
+    return t->ifmt == FMT_KV64_FP ? 1u : t->lanes;  // the fingerprint walk serves a key with one lane
+}
+
 void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block)
 {
     const uint32_t bt = t->block_threads;
-    const uint64_t groups_per_block = bt / t->cfg.tile;
+    const uint64_t groups_per_block = bt / lanes_of(t);
     uint64_t need = (n + groups_per_block - 1) / groups_per_block;
     uint64_t cap = (uint64_t)t->num_sms * t->blocks_per_sm;
     if (t->max_blocks && cap > t->max_blocks) cap = t->max_blocks;
@@ -77,11 +109,14 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     dim3 grid, block;
     launch_shape(t, a.n, grid, block);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const uint32_t b0 = t->cfg.levels[0].bucket_size, tile = t->cfg.tile;
+    const uint32_t b0 = t->cfg.levels[0].bucket_size, tile = lanes_of(t);
     cudaError_t e;
-    switch (t->cfg.format) {
-    case PG_FMT_KV64: e = launch_kv64(op, b0, tile, t->desc, a, grid, block, s); break;
-    case PG_FMT_TAGVAL16: e = launch_tagval16(op, b0, tile, t->desc, a, grid, block, s); break;
+    switch (t->ifmt) {
+    case FMT_KV64: e = launch_kv64(op, b0, tile, t->desc, a, grid, block, s); break;
+    case FMT_KV64_SPLIT: e = launch_kv64_split(op, b0, tile, t->desc, a, grid, block, s); break;
+    case FMT_TAGVAL16: e = launch_tagval16(op, b0, tile, t->desc, a, grid, block, s); break;
+    case FMT_TAGVAL16_SPLIT: e = launch_tagval16_split(op, b0, tile, t->desc, a, grid, block, s); break;
+    case FMT_KV64_FP: e = launch_kv64_fp(op, b0, tile, t->desc, a, grid, block, s); break;
     default: e = launch_tag16(op, b0, tile, t->desc, a, grid, block, s); break;
     }
     return cuda_status(e);
@@ -90,13 +125,14 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
 // occupied / tombstone counts of one level: one thread per bucket
 template <class K>
 __global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, uint64_t nb, uint32_t B,
-                                                    uint32_t bucket_bytes, K tomb, unsigned long long *out)
+                                                    uint32_t bucket_bytes, uint32_t key_stride, K tomb,
+                                                    unsigned long long *out)
 {
     uint32_t occ = 0, tmb = 0;
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (uint64_t)gridDim.x * blockDim.x) {
-        const K *k = reinterpret_cast<const K *>(base + b * bucket_bytes);
+        const unsigned char *bk = base + b * bucket_bytes;
         for (uint32_t s = 0; s < B; s++) {
-            K v = __ldcs(k + s);
+            K v = __ldcs(reinterpret_cast<const K *>(bk + s * key_stride));
             occ += v != (K)0;
             tmb += v == tomb;
         }
@@ -114,6 +150,16 @@ __global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, u
     if (threadIdx.x == 0) {
         if (sh[0]) atomicAdd(out, (unsigned long long)sh[0]);
         if (sh[1]) atomicAdd(out + 1, (unsigned long long)sh[1]);
+    }
+}
+
+// fingerprint bytes recomputed from the slots (after a level is loaded)
+__global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, unsigned char *fp, uint64_t nslots,
+                                                    uint64_t seed)
+{
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t key = *reinterpret_cast<const unsigned long long *>(base + 16 * s);
+        fp[s] = fp_of(key, murmur64a_u64(key, seed));
     }
 }
 
@@ -152,10 +198,12 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
         return PG_ERR_CUDA;
     }
     t->block_threads = 256;
-    t->blocks_per_sm = 8;
+    t->blocks_per_sm = 32;
     t->max_blocks = 0;
+    t->lanes = cfg->tile;
+    t->ifmt = internal_format(cfg);
     t->desc.nlevels = cfg->nlevels;
-    t->desc.format = cfg->format;
+    t->desc.format = t->ifmt;
     const uint32_t kb = key_bytes(cfg->format), vb = val_bytes(cfg->format);
     uint64_t s = seed;
     for (uint32_t l = 0; l < cfg->nlevels; l++) {
@@ -167,7 +215,6 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
         D.scheme = L.scheme;
         D.probe = L.probe;
         D.bucket_bytes = L.bucket_size * (kb + vb);
-        D.val_offset = L.bucket_size * kb;
         D.nbmod = make_fastmod64(nb);
         D.seed = s;
         D.seed2 = s * s;
@@ -182,6 +229,18 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
             return cuda_status(e);
         }
         D.base = static_cast<unsigned char *>(t->mem[l]);
+        D.fp = nullptr;
+        if (l == 0 && fingerprinted(cfg)) {
+            t->fp_bytes = nb * L.bucket_size;
+            e = cudaMalloc(&t->fp, t->fp_bytes);
+            if (e == cudaSuccess) e = cudaMemset(t->fp, 0, t->fp_bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                pg_table_destroy(t);
+                return cuda_status(e);
+            }
+            D.fp = static_cast<unsigned char *>(t->fp);
+        }
         s = s * s;  // recursive table gets seed*seed (base_table.cuh:124)
     }
     *out = t;
@@ -194,6 +253,7 @@ pg_status pg_table_destroy(pg_table *t)
     pg_status st = PG_OK;
     for (int l = 0; l < 2; l++)
         if (t->mem[l] && cudaFree(t->mem[l]) != cudaSuccess) st = PG_ERR_CUDA;
+    if (t->fp && cudaFree(t->fp) != cudaSuccess) st = PG_ERR_CUDA;
     free(t);
     return st;
 }
@@ -205,6 +265,7 @@ pg_status pg_table_clear(pg_table *t, pg_stream_t stream)
         cudaError_t e = cudaMemsetAsync(t->mem[l], 0, t->bytes[l], reinterpret_cast<cudaStream_t>(stream));
         if (e != cudaSuccess) return cuda_status(e);
     }
+    if (t->fp) return cuda_status(cudaMemsetAsync(t->fp, 0, t->fp_bytes, reinterpret_cast<cudaStream_t>(stream)));
     return PG_OK;
 }
 
@@ -223,16 +284,23 @@ pg_status pg_table_level_info(const pg_table *t, uint32_t level, pg_level_info *
 uint64_t pg_table_bytes(const pg_table *t)
 {
     if (!t) return 0;
-    return t->bytes[0] + t->bytes[1];
+    return t->bytes[0] + t->bytes[1] + t->fp_bytes;
 }
 
-pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks)
+pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
+                              uint32_t lanes_per_key)
 {
     if (!t) return PG_ERR_INVALID;
+    if (lanes_per_key == 0) lanes_per_key = t->cfg.tile;
+    if (!(lanes_per_key == 1 || lanes_per_key == 2 || lanes_per_key == 4 || lanes_per_key == 8 ||
+          lanes_per_key == 16))
+        return PG_ERR_INVALID;
+    if (lanes_per_key > t->cfg.levels[0].bucket_size) return PG_ERR_UNSUPPORTED;
     if (block_threads == 0) block_threads = 256;
-    if (blocks_per_sm == 0) blocks_per_sm = 8;
-    if (block_threads > 256 || block_threads % t->cfg.tile != 0) return PG_ERR_INVALID;
+    if (blocks_per_sm == 0) blocks_per_sm = 32;
+    if (block_threads > 256 || block_threads % lanes_per_key != 0) return PG_ERR_INVALID;
     if (block_threads < 32 && max_blocks != 1) return PG_ERR_INVALID;  // partial warps only for the serial shape
+    t->lanes = lanes_per_key;
     t->block_threads = block_threads;
     t->blocks_per_sm = blocks_per_sm;
     t->max_blocks = max_blocks;
@@ -271,17 +339,22 @@ pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_s
     if (blocks > cap) blocks = cap;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     auto *out = reinterpret_cast<unsigned long long *>(d_out);
+    // keys sit every key_bytes (split layout, tag-only) or every slot (interleaved)
+    const uint32_t stride = split_layout(&t->cfg) ? key_bytes(t->cfg.format)
+                                                  : key_bytes(t->cfg.format) + val_bytes(t->cfg.format);
     if (t->cfg.format == PG_FMT_KV64)
         k_count_fill<unsigned long long><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
-                                                                          ~0ULL, out);
+                                                                          stride, ~0ULL, out);
     else
         k_count_fill<unsigned short><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
-                                                                      (unsigned short)0xFFFFu, out);
+                                                                      stride, (unsigned short)0xFFFFu, out);
     return cuda_status(cudaGetLastError());
 }
 
 // Reference slot layout: slot s of bucket b at (b*B + s) * slot_bytes, the
-// key first, then the val (key_val_pair.cuh:72-74); tag-only slots hold the key.
+// key first, then the val (key_val_pair.cuh:72-74); tag-only slots hold the
+// key.  The interleaved layout is that layout already; the split layout is a
+// per-bucket permutation of it.
 pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst, uint64_t bytes)
 {
     if (!t || !host_dst || level >= t->cfg.nlevels) return PG_ERR_INVALID;
@@ -289,6 +362,8 @@ pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst,
     const uint32_t kb = key_bytes(t->cfg.format), vb = val_bytes(t->cfg.format), sb = kb + vb;
     const uint64_t nslots = D.nbmod.d * D.bucket_size;
     if (bytes != nslots * sb) return PG_ERR_INVALID;
+    if (!split_layout(&t->cfg))
+        return cuda_status(cudaMemcpy(host_dst, t->mem[level], t->bytes[level], cudaMemcpyDeviceToHost));
     std::vector<unsigned char> raw(t->bytes[level]);
     cudaError_t e = cudaMemcpy(raw.data(), t->mem[level], t->bytes[level], cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(e);
@@ -299,7 +374,7 @@ pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst,
         for (uint32_t s = 0; s < B; s++) {
             unsigned char *slot = dst + (b * B + s) * sb;
             memcpy(slot, src + s * kb, kb);
-            if (vb) memcpy(slot + kb, src + D.val_offset + s * vb, vb);
+            memcpy(slot + kb, src + B * kb + s * vb, vb);
         }
     }
     return PG_OK;
@@ -312,6 +387,14 @@ pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src,
     const uint32_t kb = key_bytes(t->cfg.format), vb = val_bytes(t->cfg.format), sb = kb + vb;
     const uint64_t nslots = D.nbmod.d * D.bucket_size;
     if (bytes != nslots * sb) return PG_ERR_INVALID;
+    if (!split_layout(&t->cfg)) {
+        cudaError_t e = cudaMemcpy(t->mem[level], host_src, t->bytes[level], cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && level == 0 && t->fp) {
+            k_rebuild_fp<<<1184, 256>>>(D.base, D.fp, nslots, D.seed);
+            e = cudaDeviceSynchronize();
+        }
+        return cuda_status(e);
+    }
     std::vector<unsigned char> raw(t->bytes[level]);
     const unsigned char *src = static_cast<const unsigned char *>(host_src);
     const uint32_t B = D.bucket_size;
@@ -320,7 +403,7 @@ pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src,
         for (uint32_t s = 0; s < B; s++) {
             const unsigned char *slot = src + (b * B + s) * sb;
             memcpy(dst + s * kb, slot, kb);
-            if (vb) memcpy(dst + D.val_offset + s * vb, slot + kb, vb);
+            memcpy(dst + B * kb + s * vb, slot + kb, vb);
         }
     }
     return cuda_status(cudaMemcpy(t->mem[level], raw.data(), t->bytes[level], cudaMemcpyHostToDevice));

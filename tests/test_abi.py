@@ -54,7 +54,7 @@ def _create(pg, cfg, seed=1):
     (lambda c: c.levels.__setitem__(0, type(c.levels[0])(64, 12, 20, 0, 0)), 4),  # level-0 bucket not compiled
     (lambda c: c.levels.__setitem__(0, type(c.levels[0])(64, 8, 9, 1, 0)), 4),   # two-choice > 4 probes
     (lambda c: setattr(c, "nlevels", 3), 1),
-    (lambda c: setattr(c, "reserved", 1), 1),
+    (lambda c: setattr(c, "flags", 6), 1),
 ])
 def test_create_rejects_bad_configs_before_touching_the_gpu(pg, mut, status):
     cfg = pg.data_structs.hash_table_64(64, bucket=8)

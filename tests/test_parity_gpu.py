@@ -20,8 +20,10 @@ pytestmark = pytest.mark.gpu
 U64MAX = (1 << 64) - 1
 
 
-def _table(pg, name, tile=None, serial=False):
+def _table(pg, name, tile=None, serial=False, layout="interleaved"):
     cfg, seed = product_config(pg, name, tile)
+    cfg.split = layout == "split"
+    cfg.fingerprints = layout == "fingerprints"
     t = pg.Table(cfg, seed)
     if serial:
         t.serial()
@@ -32,12 +34,25 @@ def _vals_for(fmt, vals):
     return vals if fmt == 0 else (vals & np.uint64(0xFFFF))
 
 
+LAYOUTS = ["interleaved", "split", "fingerprints"]
+
+
+def _layout_ok(name, layout):
+    fmt, _, levels, _ = CASES[name]
+    if layout == "fingerprints":
+        return fmt == 0 and levels[0][3] == 0  # uint64 slots, bucket_insert primary
+    return True
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_serial_matches_reference_golden_bytes(pg, name):
+def test_serial_matches_reference_golden_bytes(pg, name, layout):
     g = golden(name)
     if g is None:
         pytest.skip(f"golden fixture ref_{name}.npz not recorded yet")
-    t = _table(pg, name, serial=True)
+    if not _layout_ok(name, layout):
+        pytest.skip("layout does not apply to this table")
+    t = _table(pg, name, serial=True, layout=layout)
     d = Driver(t)
     ok = d.insert(g["keys"], g["vals"])
     assert (ok == g["insert_ok"].astype(bool)).all()
@@ -53,9 +68,12 @@ def test_serial_matches_reference_golden_bytes(pg, name):
     assert (f == g["q2_found"].astype(bool)).all() and (v == g["q2_vals"]).all()
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
 @pytest.mark.parametrize("name", sorted(CASES))
 @pytest.mark.parametrize("tile", [1, 2, 4])
-def test_serial_matches_oracle_bytes_any_tile(pg, oracle, name, tile):
+def test_serial_matches_oracle_bytes_any_tile(pg, oracle, name, tile, layout):
+    if not _layout_ok(name, layout):
+        pytest.skip("layout does not apply to this table")
     fmt = CASES[name][0]
     keys = np.concatenate([wl.keys_without_sentinels(300 + tile, 1700),
                            np.array([0, U64MAX, 0xABCD00000000FFFF, 0x10000], dtype=np.uint64)])
@@ -63,7 +81,7 @@ def test_serial_matches_oracle_bytes_any_tile(pg, oracle, name, tile):
     vals = _vals_for(fmt, wl.values_for(keys, 8, 31))
     q = np.concatenate([keys, wl.keys_without_sentinels(400, 800)])
     o = oracle_table(oracle, name)
-    t = _table(pg, name, tile=tile, serial=True)
+    t = _table(pg, name, tile=tile, serial=True, layout=layout)
     d = Driver(t)
     assert (d.insert(keys, vals) == o.insert_many(keys, vals)).all()
     for l in range(o.nlevels):
@@ -90,7 +108,7 @@ def test_parallel_matches_oracle_every_bucket_and_tile(pg, oracle, bucket, tile,
     keys = wl.keys_without_sentinels(bucket * 100 + tile, n)
     vals = _vals_for(fmt, wl.values_for(keys, 8, 5))
     q = np.concatenate([keys[: n // 2], wl.keys_without_sentinels(77, n // 2)])
-    cfg = pg.TableConfig(fmt, tile, [pg.Level(nslots, bucket, maxp, scheme, probe)])
+    cfg = pg.TableConfig(fmt, tile, [pg.Level(nslots, bucket, maxp, scheme, probe)], split=bool(tile % 2))
     t = pg.Table(cfg, 42)
     d = Driver(t)
     o = oracle.OracleTable(fmt, tile, [(nslots, bucket, maxp, scheme, probe)], 42)
@@ -221,17 +239,23 @@ def test_count_fill_and_clear(pg):
     assert not f.any()
 
 
-def test_dump_load_roundtrip(pg):
-    cfg = pg.data_structs.tcf(1 << 12, 1 << 7)
+@pytest.mark.parametrize("which", ["tcf", "ht_fingerprints"])
+def test_dump_load_roundtrip(pg, which):
+    if which == "tcf":
+        cfg = pg.data_structs.tcf(1 << 12, 1 << 7)
+    else:
+        cfg = pg.data_structs.hash_table_64(1 << 12, bucket=8)
+        cfg.fingerprints = True
     a = pg.Table(cfg, 9)
     d = Driver(a)
     keys = wl.keys_without_sentinels(8, 3400)
     d.insert(keys, wl.values_for(keys, 8, 2))
-    dumps = [a.dump_level(0), a.dump_level(1)]
+    nl = len(cfg.levels)
+    dumps = [a.dump_level(l) for l in range(nl)]
     b = pg.Table(cfg, 9)
-    b.load_level(0, dumps[0])
-    b.load_level(1, dumps[1])
-    assert b.dump_level(0) == dumps[0] and b.dump_level(1) == dumps[1]
+    for l in range(nl):
+        b.load_level(l, dumps[l])
+    assert all(b.dump_level(l) == dumps[l] for l in range(nl))
     fa, va = d.query(keys)
     fb, vb = Driver(b).query(keys)
     assert (fa == fb).all() and (va == vb).all()
@@ -271,3 +295,38 @@ def test_unaligned_and_ragged_batches(pg, oracle):
     f, v = Driver(t).query(keys[3:])
     fo, vo = o.query_many(keys[3:])
     assert (f == fo).all() and (v == vo).all()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+@pytest.mark.parametrize("tile", [1, 2, 4])
+@pytest.mark.parametrize("bucket", [4, 8, 16, 32])
+def test_layouts_match_oracle(pg, oracle, layout, tile, bucket):
+    """Both bucket layouts give the oracle's results on every key both runs
+    placed, including sentinel keys, for insert, query, remove and re-query."""
+    nslots = 1 << 15
+    n = int(0.9 * nslots)
+    keys = wl.keys_without_sentinels(LAYOUTS.index(layout) * 10 + tile + bucket, n)
+    vals = wl.values_for(keys, 8, 6)
+    q = np.concatenate([keys[: n // 2], wl.keys_without_sentinels(88, n // 2), np.array([0, U64MAX], dtype=np.uint64)])
+    cfg = pg.data_structs.hash_table_64(nslots, tile=min(tile, bucket), bucket=bucket)
+    cfg.split = layout == "split"
+    cfg.fingerprints = layout == "fingerprints"
+    t = pg.Table(cfg, 42)
+    d = Driver(t)
+    o = oracle.OracleTable(0, 4, [(nslots, bucket, 20, 0, 0)], 42)
+    ok, oko = d.insert(keys, vals), o.insert_many(keys, vals)
+    both = np.concatenate([ok[: n // 2] & oko[: n // 2], np.ones(len(q) - n // 2, dtype=bool)])
+    f, v = d.query(q)
+    fo, vo = o.query_many(q)
+    assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
+    assert (f[: n // 2] == ok[: n // 2]).all()
+    ridx = wl.fisher_yates_half(n, 3)
+    assert (d.remove(keys[ridx]) == ok[ridx]).all()
+    o.remove_many(keys[ridx])
+    f, v = d.query(q)
+    fo, vo = o.query_many(q)
+    # after removes, the sentinel keys read whichever tombstone / empty slot their
+    # bucket holds, which depends on placement order (in the reference too)
+    both[-2:] = False
+    assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
+    assert t.get_fill(0)[1] == int(ok[ridx].sum())
