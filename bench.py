@@ -37,7 +37,7 @@ NSLOTS = 1 << 26
 BUCKET = 8
 TILE = 4          # the reference's Partition_Size for this table (semantics)
 LANES = 2         # lanes per key the kernels use (launch shape; results do not depend on it)
-SPLIT = True      # keys then values inside each bucket
+LAYOUT = "fingerprints"  # reference {key,val} slots + an L2-resident fingerprint byte per slot
 BLOCK_THREADS = 256
 BLOCKS_PER_SM = 32
 PROBES = 20
@@ -143,7 +143,8 @@ def run_ours(args, rank, world):
     found = torch.empty(nq, dtype=torch.uint8, device=dev)
     qv = torch.empty(nq, dtype=torch.int64, device=dev)
     cfg = pg.data_structs.hash_table_64(NSLOTS, tile=TILE, bucket=BUCKET, max_probes=PROBES)
-    cfg.split = SPLIT
+    cfg.split = args.layout == "split"
+    cfg.fingerprints = args.layout == "fingerprints"
     table = pg.Table(cfg, SEED)
     table.set_launch(BLOCK_THREADS, BLOCKS_PER_SM, 0, LANES)
     stream = torch.cuda.current_stream()
@@ -217,8 +218,9 @@ def run_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded splitmix64 keys)",
         "config": {"workload": WORKLOAD, "slots": NSLOTS, "inserts": n, "queries": nq,
-                   "launch": {"lanes_per_key": LANES, "block_threads": BLOCK_THREADS,
-                              "blocks_per_sm": BLOCKS_PER_SM, "bucket_layout": "split" if SPLIT else "interleaved"},
+                   "launch": {"lanes_per_key": 1 if args.layout == "fingerprints" else LANES,
+                              "block_threads": BLOCK_THREADS, "blocks_per_sm": BLOCKS_PER_SM,
+                              "bucket_layout": args.layout},
                    "parallelism": f"independent table per GPU x{world}",
                    "l2": "inputs larger than L2 (1 GiB table, 126 MB L2)"},
         "roofline": {"bound": "hbm", "kernel": f"bulk_{dom}", "achieved": round(achieved, 1),
@@ -451,6 +453,7 @@ def main():
     ap.add_argument("--ref-target", choices=["cpu", "cuda"], default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--layout", choices=["fingerprints", "interleaved", "split"], default=LAYOUT)
     ap.add_argument("--slots-log2", type=int, default=26,
                     help="table size (default 26 = the benchmark workload; smaller only for profiling captures)")
     args = ap.parse_args()

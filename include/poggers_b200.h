@@ -169,6 +169,76 @@ pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst,
 pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes);
 
 /* ---------------------------------------------------------------------------
+ * Multi-table batches: many requests over many tables in one persistent launch.
+ *
+ * No counterpart in the reference, which launches one kernel per batch per
+ * table (tests/src/test_mhm_tcf.cu:603-685); each request here is what one
+ * such launch would do, and its results equal that launch's.  Requests in one
+ * run execute concurrently, so -- as with separate launches -- requests that
+ * conflict on one table (an insert or remove with anything else on that
+ * table) belong in separate runs (stream-ordered).
+ * --------------------------------------------------------------------------- */
+enum { PG_OP_INSERT = 0, PG_OP_QUERY = 1, PG_OP_REMOVE = 2 };
+
+typedef struct pg_op_desc {
+    uint32_t table;  /* index into the batch's table list */
+    uint32_t op;     /* PG_OP_* */
+    uint64_t offset; /* first key (and value / result) index of the request */
+    uint64_t count;  /* keys in the request */
+} pg_op_desc;
+
+typedef struct pg_batch pg_batch;
+
+/* Register tables for batched runs.  All must share format, layout flags,
+ * level-0 bucket size and scheme, and whether they have a backing level.
+ * max_ops bounds the requests of one run (scratch is sized for it). */
+pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t max_ops, pg_batch **out);
+pg_status pg_batch_destroy(pg_batch *b);
+pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t lanes_per_key);
+/* Run d_ops[0 .. *d_nops) (both device memory, so one captured CUDA graph can be
+ * replayed with new requests).  Keys, values and per-key flags are indexed by
+ * the requests' offsets; d_op_counts[j] (optional) += hits of query / remove
+ * request j, or failures of insert request j. */
+pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_nops, const uint64_t *d_keys,
+                       const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
+                       pg_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Continuous-batching server over resident tables (no counterpart in the
+ * reference).  Requests from host memory are packed by a worker thread into
+ * waves of pg_batch_run calls; up to two waves are on the GPU at once, and
+ * requests that arrive meanwhile join the next wave.  Per table, requests
+ * complete in submission order and results equal running them one at a
+ * time in that order.  A request's host buffers must stay valid until it
+ * completes.
+ * --------------------------------------------------------------------------- */
+typedef struct pg_server pg_server;
+
+typedef struct pg_server_config {
+    uint64_t hbm_budget_bytes;  /* tables are admitted while their bytes fit */
+    uint64_t max_wave_keys;     /* keys staged per wave (also the largest request) */
+    uint32_t max_wave_requests; /* requests per wave */
+    uint32_t reserved;
+} pg_server_config;
+
+pg_status pg_server_create(const pg_server_config *cfg, pg_server **out);
+pg_status pg_server_destroy(pg_server *s);
+/* Create a resident table; PG_ERR_FULL when it would exceed the HBM budget. */
+pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t seed, uint32_t *table_id);
+/* Release a table and its share of the budget (none of its requests may be pending). */
+pg_status pg_server_drop_table(pg_server *s, uint32_t table_id);
+pg_table *pg_server_table(pg_server *s, uint32_t table_id);
+uint64_t pg_server_bytes_in_use(pg_server *s);
+/* Queue one request; values typed as for pg_bulk_*.  h_vals_out / h_flags optional. */
+pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const uint64_t *h_keys, const void *h_vals,
+                           uint64_t n, void *h_vals_out, uint8_t *h_flags, uint64_t *request_id);
+/* Collect a finished request: PG_OK (count = hits or failures, latency in
+ * seconds from submit to completion), or PG_ERR_TIMEOUT if it is still
+ * running and wait == 0.  A request is collected once. */
+pg_status pg_server_poll(pg_server *s, uint64_t request_id, int wait, uint64_t *count, double *latency_s);
+pg_status pg_server_stats(pg_server *s, uint64_t *waves, uint64_t *keys);
+
+/* ---------------------------------------------------------------------------
  * Slab allocator: fixed-size objects from slabs of 4096.
  *
  * Replaces one_size_slab_allocator<N> (allocators/slab_one_size.cuh:58-659):

@@ -98,25 +98,37 @@ enum probe_kind : uint32_t { PROBE_DOUBLE = 0, PROBE_LINEAR = 1, PROBE_P2 = 2, P
 constexpr uint64_t kProbeEnd = ~0ULL;
 
 struct probe_seq {
-    uint64_t h1, h2;
+    uint64_t h1, h2, key, seed2;
     uint32_t kind;
+    bool have2;
 
-    PG_HD void begin(uint32_t k, uint64_t key, uint64_t tag, uint64_t seed, uint64_t seed2)
+    // h1 now; the second hash of double / power-of-two probing only when a
+    // probe past the first is asked for (most operations stop at probe 0)
+    PG_HD void begin(uint32_t k, uint64_t ky, uint64_t tag, uint64_t seed, uint64_t s2)
     {
         kind = k;
-        h1 = murmur64a_u64(key, seed);
-        if (k == PROBE_DOUBLE || k == PROBE_P2) h2 = murmur64a_u64(key, seed2);
-        else if (k == PROBE_XOR_P2) h2 = h1 ^ (tag * 0x5bd1e995ULL);
-        else h2 = 1;
+        key = ky;
+        seed2 = s2;
+        h1 = murmur64a_u64(ky, seed);
+        have2 = !(k == PROBE_DOUBLE || k == PROBE_P2);
+        h2 = (k == PROBE_XOR_P2) ? (h1 ^ (tag * 0x5bd1e995ULL)) : 1;
+    }
+    PG_HD uint64_t second()
+    {
+        if (!have2) {
+            h2 = murmur64a_u64(key, seed2);
+            have2 = true;
+        }
+        return h2;
     }
     // raw probe value i (i < max_probes)
-    PG_HD uint64_t at(uint32_t i) const
+    PG_HD uint64_t at(uint32_t i)
     {
         if (i == 0) return h1;
         switch (kind) {
-        case PROBE_DOUBLE: return h1 + (uint64_t)i * h2;
+        case PROBE_DOUBLE: return h1 + (uint64_t)i * second();
         case PROBE_LINEAR: return h1 + (uint64_t)i;
-        default: return h2;  // p2 and xor_p2: the second choice
+        default: return second();  // p2 and xor_p2: the second choice
         }
     }
 };

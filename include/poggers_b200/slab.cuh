@@ -30,8 +30,13 @@ namespace pg {
 constexpr uint32_t kSlabObjects = 4096;   // objects per slab (64 words x 64 bits)
 constexpr uint32_t kSlabWords = 64;
 constexpr uint32_t kSlabCursors = 256;    // per-SM cursors, indexed by %smid & 255
-constexpr uint32_t kSlabMaxAttempts = 25; // claims that find nothing (SLAB_ONE_SIZE_MAX_ATTEMPTS)
-constexpr uint32_t kSlabMaxMoves = 256;   // moves of an SM to another slab within one call
+// Bounds of one malloc call.  The reference gives up after 25 attempts
+// (SLAB_ONE_SIZE_MAX_ATTEMPTS, slab_one_size.cuh:20); here a claim that finds
+// nothing because other warps took the bits first, and a move to another slab,
+// are bounded separately and more loosely, so that NULL means the pool is full
+// rather than contended.
+constexpr uint32_t kSlabMaxAttempts = 64;
+constexpr uint32_t kSlabMaxMoves = 1024;
 
 struct slab_desc {
     unsigned char *pool;           // nslabs * 4096 objects of `size` bytes

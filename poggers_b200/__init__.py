@@ -62,6 +62,11 @@ class _LevelInfo(C.Structure):
                 ("seed", C.c_uint64), ("d_buckets", C.c_void_p)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_wave_keys", C.c_uint64),
+                ("max_wave_requests", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class _SlabInfo(C.Structure):
     _fields_ = [("pool", C.c_void_p), ("pool_bytes", C.c_uint64), ("object_bytes", C.c_uint64),
                 ("capacity", C.c_uint64), ("nslabs", C.c_uint64), ("d_stats", C.c_void_p)]
@@ -77,7 +82,11 @@ EXPORTED = (
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
+    "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run",
+    "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
+    "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
 )
+PG_OP_INSERT, PG_OP_QUERY, PG_OP_REMOVE = 0, 1, 2
 
 
 def lib() -> C.CDLL:
@@ -142,6 +151,32 @@ def lib() -> C.CDLL:
     L.pg_slab_set_bulk_malloc.argtypes = [V, P, U64, P, P, P]
     L.pg_slab_set_bulk_free.restype = C.c_int
     L.pg_slab_set_bulk_free.argtypes = [V, P, U64, P, P]
+    L.pg_batch_create.restype = C.c_int
+    L.pg_batch_create.argtypes = [C.POINTER(V), U32, U32, C.POINTER(V)]
+    L.pg_batch_destroy.restype = C.c_int
+    L.pg_batch_destroy.argtypes = [V]
+    L.pg_batch_set_launch.restype = C.c_int
+    L.pg_batch_set_launch.argtypes = [V, U32, U32, U32]
+    L.pg_batch_run.restype = C.c_int
+    L.pg_batch_run.argtypes = [V, P, P, P, P, P, P, P, P]
+    L.pg_server_create.restype = C.c_int
+    L.pg_server_create.argtypes = [C.POINTER(_ServerConfig), C.POINTER(V)]
+    L.pg_server_destroy.restype = C.c_int
+    L.pg_server_destroy.argtypes = [V]
+    L.pg_server_add_table.restype = C.c_int
+    L.pg_server_add_table.argtypes = [V, C.POINTER(_TableConfig), U64, C.POINTER(U32)]
+    L.pg_server_drop_table.restype = C.c_int
+    L.pg_server_drop_table.argtypes = [V, U32]
+    L.pg_server_table.restype = V
+    L.pg_server_table.argtypes = [V, U32]
+    L.pg_server_bytes_in_use.restype = U64
+    L.pg_server_bytes_in_use.argtypes = [V]
+    L.pg_server_submit.restype = C.c_int
+    L.pg_server_submit.argtypes = [V, U32, U32, P, P, U64, P, P, C.POINTER(U64)]
+    L.pg_server_poll.restype = C.c_int
+    L.pg_server_poll.argtypes = [V, U64, C.c_int, C.POINTER(U64), C.POINTER(C.c_double)]
+    L.pg_server_stats.restype = C.c_int
+    L.pg_server_stats.argtypes = [V, C.POINTER(U64), C.POINTER(U64)]
     L.pg_host_murmur64a.restype = U64
     L.pg_host_murmur64a.argtypes = [U64, U64]
     L.pg_host_fastmod.restype = U64
@@ -478,3 +513,113 @@ class allocators:
         def bulk_free(self, ptrs, bad_count=None, stream=None) -> None:
             _check(lib().pg_slab_set_bulk_free(self._h, _ptr(ptrs), ptrs.numel(), _ptr(bad_count), _stream(stream)),
                    "pg_slab_set_bulk_free")
+
+
+# ---------------------------------------------------------------- multi-table batches
+def pack_ops(ops) -> "np.ndarray":
+    """[(table, op, offset, count), ...] -> int64 array laid out as pg_op_desc (24 bytes each)."""
+    import numpy as np
+    a = np.zeros((len(ops), 3), dtype=np.uint64)
+    for i, (t, op, off, cnt) in enumerate(ops):
+        a[i, 0] = np.uint64(t) | (np.uint64(op) << np.uint64(32))
+        a[i, 1] = off
+        a[i, 2] = cnt
+    return a.view(np.int64).reshape(-1)
+
+
+class Batch:
+    """Tables registered for multi-table runs (pg_batch_*)."""
+
+    def __init__(self, tables: list, max_ops: int):
+        arr = (C.c_void_p * len(tables))(*[t.handle.value for t in tables])
+        h = C.c_void_p()
+        _check(lib().pg_batch_create(arr, len(tables), max_ops, C.byref(h)), "pg_batch_create")
+        self._h = h
+        self.tables = list(tables)
+        self.max_ops = max_ops
+
+    def free(self) -> None:
+        if getattr(self, "_h", None):
+            _check(lib().pg_batch_destroy(self._h), "pg_batch_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def set_launch(self, block_threads: int = 0, blocks_per_sm: int = 0, lanes_per_key: int = 0) -> None:
+        _check(lib().pg_batch_set_launch(self._h, block_threads, blocks_per_sm, lanes_per_key), "pg_batch_set_launch")
+
+    def run(self, ops, nops, keys, vals_in=None, vals_out=None, flags=None, op_counts=None, stream=None) -> None:
+        """ops: int64 device tensor from pack_ops; nops: int32 device tensor holding the request count."""
+        _check(lib().pg_batch_run(self._h, _ptr(ops), _ptr(nops), _ptr(keys), _ptr(vals_in), _ptr(vals_out),
+                                  _ptr(flags), _ptr(op_counts), _stream(stream)), "pg_batch_run")
+
+
+# ---------------------------------------------------------------- serving
+class Server:
+    """Continuous-batching server over resident tables (pg_server_*).
+
+    submit() takes numpy arrays (kept alive until the request is collected);
+    poll(rid, wait) returns (count, latency_s) or None while it is running."""
+
+    def __init__(self, hbm_budget_bytes: int, max_wave_keys: int = 1 << 22, max_wave_requests: int = 4096):
+        cfg = _ServerConfig(hbm_budget_bytes, max_wave_keys, max_wave_requests, 0)
+        h = C.c_void_p()
+        _check(lib().pg_server_create(C.byref(cfg), C.byref(h)), "pg_server_create")
+        self._h = h
+        self._live = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _check(lib().pg_server_destroy(self._h), "pg_server_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_table(self, config: "TableConfig", seed: int) -> int | None:
+        """Table id, or None when the HBM budget is exhausted (PG_ERR_FULL)."""
+        c = config.c()
+        tid = C.c_uint32()
+        st = lib().pg_server_add_table(self._h, C.byref(c), seed, C.byref(tid))
+        if st == PG_ERR_FULL:
+            return None
+        _check(st, "pg_server_add_table")
+        return tid.value
+
+    def drop_table(self, tid: int) -> None:
+        _check(lib().pg_server_drop_table(self._h, tid), "pg_server_drop_table")
+
+    def bytes_in_use(self) -> int:
+        return lib().pg_server_bytes_in_use(self._h)
+
+    def submit(self, tid: int, op: int, keys, vals=None, vals_out=None, flags=None) -> int:
+        import numpy as np
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        rid = C.c_uint64()
+        _check(lib().pg_server_submit(self._h, tid, op, keys.ctypes.data, None if vals is None else vals.ctypes.data,
+                                      len(keys), None if vals_out is None else vals_out.ctypes.data,
+                                      None if flags is None else flags.ctypes.data, C.byref(rid)), "pg_server_submit")
+        self._live[rid.value] = (keys, vals, vals_out, flags)
+        return rid.value
+
+    def poll(self, rid: int, wait: bool = False):
+        cnt = C.c_uint64()
+        lat = C.c_double()
+        st = lib().pg_server_poll(self._h, rid, 1 if wait else 0, C.byref(cnt), C.byref(lat))
+        if st == PG_ERR_TIMEOUT:
+            return None
+        _check(st, "pg_server_poll")
+        self._live.pop(rid, None)
+        return cnt.value, lat.value
+
+    def stats(self) -> tuple[int, int]:
+        w, k = C.c_uint64(), C.c_uint64()
+        _check(lib().pg_server_stats(self._h, C.byref(w), C.byref(k)), "pg_server_stats")
+        return w.value, k.value

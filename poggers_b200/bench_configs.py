@@ -1,0 +1,318 @@
+"""Measurements of the secondary workloads (the headline is bench.py).
+
+    python -m poggers_b200.bench_configs --config 1   # plain TCF, 2^22 slots
+    python -m poggers_b200.bench_configs --config 3   # 1024 TCFs: batched vs per-table launches
+    python -m poggers_b200.bench_configs --config 4   # served request stream vs plain per-request path
+
+Each prints one JSON line.  All inputs are seeded synthetic keys.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+import poggers_b200 as pg
+from poggers_b200 import workload as wl
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64 if a.dtype == np.uint64 else np.int16)).cuda()
+
+
+def _events(n):
+    import torch
+    return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+
+
+# ---------------------------------------------------------------- config 1
+def config1(args):
+    """Plain TCF: 2^22 slots of 16-bit tags (+16-bit values), buckets of 16, 1%
+    backing table; insert to 0.85 load; query the inserted keys and 2^22 fresh."""
+    import torch
+    n0 = 1 << 22
+    n = int(0.85 * n0)
+    keys = wl.keys_without_sentinels(42, n)
+    fresh = wl.keys_without_sentinels(4242, n0)
+    vals = wl.values_for(keys, 2, 49)
+    cfg = pg.data_structs.tcf(n0, n0 // 100)
+    cfg.split = True
+    t = pg.Table(cfg, 42)
+    t.set_launch(256, 32, 0, 1)
+    dk, dv, df = _dev(keys), _dev(vals), _dev(fresh)
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    f1 = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    f2 = torch.zeros(n0, dtype=torch.uint8, device="cuda")
+    ins, qp, qn = [], [], []
+    for step in range(args.steps + 3):
+        t.clear()
+        e = _events(4)
+        e[0].record()
+        t.bulk_insert(dk, dv, ok)
+        e[1].record()
+        t.bulk_query(dk, None, f1)
+        e[2].record()
+        t.bulk_query(df, None, f2)
+        e[3].record()
+        torch.cuda.synchronize()
+        if step >= 3:
+            ins.append(e[0].elapsed_time(e[1]))
+            qp.append(e[1].elapsed_time(e[2]))
+            qn.append(e[2].elapsed_time(e[3]))
+    okn = ok.cpu().numpy().astype(bool)
+    fn = int((~f1.cpu().numpy().astype(bool) & okn).sum())
+    fp = float(f2.cpu().numpy().astype(bool).mean())
+    ms = np.median(ins) + np.median(qp) + np.median(qn)
+    return {"config": 1, "workload": "TCF 2^22 slots (16-bit tag+val, bucket 16) + 1% backing, 0.85 load",
+            "insert_mops": round(n / np.median(ins) / 1e3, 1),
+            "query_pos_mops": round(n / np.median(qp) / 1e3, 1),
+            "query_neg_mops": round(n0 / np.median(qn) / 1e3, 1),
+            "mops_insert_query": round((n + n + n0) / ms / 1e3, 1),
+            "insert_failures": int((~okn).sum()), "false_negatives": fn, "fp_rate": fp,
+            "roofline_note": "table is 16 MiB, L2-resident: bound by L2, not HBM"}
+
+
+# ---------------------------------------------------------------- config 3
+def config3(args):
+    """1024 TCFs, slot counts log-uniform in [2^12, 2^20], each filled to 0.9.
+    All inserts in one batched launch, then all queries (half inserted, half
+    absent) in another, replayed from a captured CUDA graph; against 1024
+    per-table launches per phase."""
+    import torch
+    rng = np.random.default_rng(3)
+    ntab = args.tables
+    sizes = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 20), ntab)).astype(np.int64)
+    bucket = args.bucket
+    tables = []
+    for i, n in enumerate(sizes):
+        cfg = pg.data_structs.tcf(int(n), max(int(n) // 20, 64), bucket=bucket)
+        tables.append(pg.Table(cfg, 1000 + i))
+    counts = (0.9 * sizes).astype(np.int64)
+    keys = [wl.keys_without_sentinels(77_000 + i, int(c)) for i, c in enumerate(counts)]
+    qkeys = [np.concatenate([k[: len(k) // 2], wl.keys_without_sentinels(99_000 + i, len(k) - len(k) // 2)])
+             for i, k in enumerate(keys)]
+    ins_all, q_all = np.concatenate(keys), np.concatenate(qkeys)
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    vals = wl.values_for(ins_all, 2, 5)
+    dk, dv, dq = _dev(ins_all), _dev(vals), _dev(q_all)
+    N = len(ins_all)
+    ok = torch.zeros(N, dtype=torch.uint8, device="cuda")
+    found = torch.zeros(N, dtype=torch.uint8, device="cuda")
+    lanes = args.lanes
+
+    # plain path: one launch per table per phase
+    for t in tables:
+        t.set_launch(256, 8, 0, lanes)
+
+    def plain():
+        for t in tables:
+            t.clear()
+        for i, t in enumerate(tables):
+            a, b = int(offs[i]), int(offs[i + 1])
+            t.bulk_insert(dk[a:b], dv[a:b], ok[a:b])
+        for i, t in enumerate(tables):
+            a, b = int(offs[i]), int(offs[i + 1])
+            t.bulk_query(dq[a:b], None, found[a:b])
+
+    # batched path: one run per phase, captured once
+    batch = pg.Batch(tables, max_ops=ntab)
+    batch.set_launch(256, args.blocks_per_sm, lanes)
+    ins_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_INSERT, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
+    q_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_QUERY, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
+    d_n = torch.tensor([ntab], dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+
+    def batched_run(stream):
+        batch.run(ins_ops, d_n, dk, dv, None, ok, None, stream)
+        batch.run(q_ops, d_n, dq, None, None, found, None, stream)
+
+    def clear_all(stream):
+        for t in tables:
+            t.clear(stream)
+
+    with torch.cuda.stream(s):
+        clear_all(s)
+        batched_run(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        clear_all(s)
+        batched_run(s)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events(2)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    plain_ms = timed(plain, args.steps)
+    graph_ms = timed(g.replay, args.steps)
+    g.replay()
+    torch.cuda.synchronize()
+    okn = ok.cpu().numpy().astype(bool)
+    fnd = found.cpu().numpy().astype(bool)
+    fn_total = 0
+    fp_total = 0
+    for i in range(ntab):
+        a, b = int(offs[i]), int(offs[i + 1])
+        half = (b - a) // 2
+        fn_total += int((~fnd[a:a + half] & okn[a:a + half]).sum())
+        fp_total += int(fnd[a + half:b].sum())
+    ops = 2 * N
+    del g
+    batch.free()
+    return {"config": 3, "workload": f"{ntab} TCFs, slots log-uniform [2^12, 2^20] (total {int(sizes.sum())}), 0.9 load, "
+                                     f"bucket {bucket}, lanes/key {lanes}",
+            "keys": int(N), "plain_ms": round(plain_ms, 3), "batched_graph_ms": round(graph_ms, 3),
+            "plain_mops": round(ops / plain_ms / 1e3, 1), "batched_mops": round(ops / graph_ms / 1e3, 1),
+            "speedup": round(plain_ms / graph_ms, 2), "insert_failures": int((~okn).sum()),
+            "false_negatives": fn_total, "fp_rate": fp_total / max(1, N - N // 2)}
+
+
+# ---------------------------------------------------------------- config 4
+def _request_stream(rng, ntab, nreq, kinds, zipf_a=0.99, max_log2=16):
+    w = 1.0 / np.arange(1, ntab + 1) ** zipf_a
+    w /= w.sum()
+    tables = rng.choice(ntab, size=nreq, p=w)
+    ops = rng.choice(3, size=nreq, p=[0.3, 0.6, 0.1])
+    sizes = np.floor(2 ** rng.uniform(0, max_log2, nreq)).astype(np.int64)
+    return tables, ops, sizes
+
+
+def config4(args):
+    """Served request stream: resident tables (TCFs and uint64 double-hash tables),
+    Zipf(0.99) table choice, Poisson arrivals, insert/query/delete 30/60/10,
+    request sizes 2^U keys with U ~ Uniform[0, 16].  Reports served Mops/s and
+    p50/p99 latency at each offered rate, and the plain per-request path."""
+    import torch
+    rng = np.random.default_rng(4)
+    ntab = args.tables
+    budget = int(args.budget_gb * (1 << 30))
+    per = budget // ntab
+    kinds = ["tcf" if i % 2 else "ht" for i in range(ntab)]
+    srv = pg.Server(hbm_budget_bytes=budget, max_wave_keys=1 << 20, max_wave_requests=4096)
+    plain_tables = []
+    ids = []
+    for i, k in enumerate(kinds):
+        if k == "ht":
+            n = per // 17  # 16 B slots + 1 B fingerprints
+            cfg = pg.data_structs.hash_table_64(n, bucket=8)
+            cfg.fingerprints = True
+        else:
+            n = per // 4
+            cfg = pg.data_structs.tcf(int(n * 0.95), int(n * 0.05) // 1)
+        tid = srv.add_table(cfg, 500 + i)
+        if tid is None:
+            break
+        ids.append((tid, k, n))
+    nt = len(ids)
+    # per-table key streams: inserts take fresh keys, queries half known / half absent, deletes known keys
+    nreq = args.requests
+    tsel, ops, sizes = _request_stream(rng, nt, nreq, kinds)
+    fresh_pos = np.zeros(nt, dtype=np.int64)
+    reqs = []
+    for t, op, n in zip(tsel, ops, sizes):
+        n = int(max(1, n))
+        if op == 0:
+            k = wl.splitmix64(900_000 + int(t), n, int(fresh_pos[t]))
+            fresh_pos[t] += n
+        elif op == 1:
+            # half a run of keys inserted earlier (the table's key stream), half never inserted
+            m = min(n // 2, int(fresh_pos[t]))
+            st = int(rng.integers(0, int(fresh_pos[t]) - m + 1)) if m else 0
+            pos = wl.splitmix64(900_000 + int(t), m, st)
+            k = np.concatenate([pos, wl.splitmix64(5_000_000 + int(t), n - m, int(rng.integers(1 << 40)))])
+        else:
+            m = min(max(1, n // 4), int(fresh_pos[t]))
+            st = int(rng.integers(0, int(fresh_pos[t]) - m + 1)) if m else 0
+            k = wl.splitmix64(900_000 + int(t), m, st)
+            if m == 0:
+                continue
+        reqs.append((ids[t][0], int(op), k, ids[t][1]))
+    total_keys = sum(len(r[2]) for r in reqs)
+    results = {}
+    for rate in args.rates:
+        gaps = rng.exponential(1.0 / rate, len(reqs))
+        arrive = np.cumsum(gaps)
+        outs = []
+        t0 = time.perf_counter()
+        rids = []
+        for (tid, op, k, kind), at in zip(reqs, arrive):
+            while time.perf_counter() - t0 < at:
+                pass
+            vb = 8 if kind == "ht" else 2
+            vals = wl.values_for(k, vb, 1) if op == 0 else None
+            vout = np.zeros(len(k), dtype=np.uint64 if vb == 8 else np.uint16) if op == 1 else None
+            rids.append(srv.submit(tid, op, k, vals, vout, None))
+            outs.append((vals, vout))
+        lats = [srv.poll(r, wait=True)[1] for r in rids]
+        el = time.perf_counter() - t0
+        results[str(rate)] = {"offered_req_s": rate, "achieved_mops": round(total_keys / el / 1e6, 1),
+                              "p50_ms": round(1e3 * float(np.percentile(lats, 50)), 3),
+                              "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3)}
+    waves, _ = srv.stats()
+    in_use = srv.bytes_in_use()
+    # plain path: the same requests one launch each, in order, from host buffers
+    plain = []
+    for tid, k, n in ids:
+        plain.append(pg.Table(srv_config_of(k, n), 1))
+    t0 = time.perf_counter()
+    for tid, op, k, kind in reqs[: args.plain_requests]:
+        t = plain[tid]
+        dk = _dev(k)
+        flags = torch.zeros(len(k), dtype=torch.uint8, device="cuda")
+        if op == 0:
+            vb = 8 if kind == "ht" else 2
+            t.bulk_insert(dk, _dev(wl.values_for(k, vb, 1)), flags)
+        elif op == 1:
+            t.bulk_query(dk, None, flags)
+        else:
+            t.bulk_remove(dk, flags)
+        flags.cpu()
+    pl = time.perf_counter() - t0
+    plain_keys = sum(len(r[2]) for r in reqs[: args.plain_requests])
+    srv.close()
+    return {"config": 4, "workload": f"{nt} resident tables ({args.budget_gb} GB budget), Zipf 0.99, Poisson arrivals, "
+                                     f"insert/query/delete 30/60/10, 2^U keys U~U[0,16], {nreq} requests",
+            "tables": nt, "bytes_in_use": int(in_use), "requests": nreq, "keys": int(total_keys), "waves": int(waves),
+            "served": results, "plain_mops": round(plain_keys / pl / 1e6, 1),
+            "plain_requests": args.plain_requests}
+
+
+def srv_config_of(kind, n):
+    if kind == "ht":
+        cfg = pg.data_structs.hash_table_64(n, bucket=8)
+        cfg.fingerprints = True
+        return cfg
+    return pg.data_structs.tcf(int(n * 0.95), int(n * 0.05))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", type=int, required=True)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--tables", type=int, default=1024)
+    ap.add_argument("--bucket", type=int, default=16)
+    ap.add_argument("--lanes", type=int, default=1)
+    ap.add_argument("--blocks-per-sm", type=int, default=8)
+    ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--requests", type=int, default=4000)
+    ap.add_argument("--plain-requests", type=int, default=1000)
+    ap.add_argument("--rates", type=float, nargs="+", default=[2000.0, 8000.0, 32000.0])
+    a = ap.parse_args()
+    import torch
+    torch.cuda.init()
+    fn = {1: config1, 3: config3, 4: config4}[a.config]
+    print(json.dumps(fn(a)))
+
+
+if __name__ == "__main__":
+    main()

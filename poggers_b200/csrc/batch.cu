@@ -1,0 +1,176 @@
+// batch.cu -- C ABI of the multi-table batch path (plan + persistent kernel).
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <cuda_runtime.h>
+
+#include "poggers_b200.h"
+#include "batch_kernels.cuh"
+#include "table_internal.h"
+
+using namespace pg;
+
+struct pg_batch {
+    uint32_t ntables;
+    uint32_t max_ops;
+    uint32_t ifmt, bucket, scheme;
+    bool backing;
+    table_desc *d_tables;
+    unsigned long long *d_scratch;  // chunk_start[max_ops + 1] then the work counter
+    int num_sms;
+    uint32_t block_threads, blocks_per_sm, lanes;
+};
+
+namespace pg {
+
+__global__ void __launch_bounds__(1024) k_batch_plan(batch_args a)
+{
+    __shared__ unsigned long long carry;
+    __shared__ unsigned long long warp_sums[32];
+    uint32_t nops = *a.nops;
+    if (nops > a.max_ops) nops = a.max_ops;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        *a.work = 0;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < nops; base += blockDim.x) {
+        const uint32_t j = base + threadIdx.x;
+        unsigned long long v = 0;
+        if (j < nops) v = (a.ops[j].count + kBatchChunk - 1) / kBatchChunk;
+        // inclusive scan in the warp, then across warps
+        unsigned long long x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if ((int)lane >= o) w += y;
+            }
+            warp_sums[lane] = w;  // inclusive prefix of warp totals
+        }
+        __syncthreads();
+        const unsigned long long before = carry + (warp ? warp_sums[warp - 1] : 0) + x - v;
+        if (j < nops) a.chunk_start[j] = before;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a.chunk_start[nops] = carry;
+}
+
+}  // namespace pg
+
+extern "C" {
+
+pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t max_ops, pg_batch **out)
+{
+    if (!out || !tables || ntables == 0 || max_ops == 0) return PG_ERR_INVALID;
+    *out = nullptr;
+    const pg_table *t0 = tables[0];
+    if (!t0) return PG_ERR_INVALID;
+    for (uint32_t i = 1; i < ntables; i++) {
+        const pg_table *t = tables[i];
+        // one kernel instantiation serves the batch: same format, bucket, scheme and depth
+        if (!t || t->ifmt != t0->ifmt || t->cfg.levels[0].bucket_size != t0->cfg.levels[0].bucket_size ||
+            t->cfg.levels[0].scheme != t0->cfg.levels[0].scheme || (t->cfg.nlevels > 1) != (t0->cfg.nlevels > 1) ||
+            t->device != t0->device)
+            return PG_ERR_UNSUPPORTED;
+    }
+    pg_batch *b = (pg_batch *)calloc(1, sizeof(pg_batch));
+    if (!b) return PG_ERR_NOMEM;
+    b->ntables = ntables;
+    b->max_ops = max_ops;
+    b->ifmt = t0->ifmt;
+    b->bucket = t0->cfg.levels[0].bucket_size;
+    b->scheme = t0->cfg.levels[0].scheme;
+    b->backing = t0->cfg.nlevels > 1;
+    b->num_sms = t0->num_sms;
+    b->block_threads = 256;
+    b->blocks_per_sm = 8;
+    b->lanes = pg_table_lanes(t0);
+    table_desc *h = (table_desc *)malloc(sizeof(table_desc) * ntables);
+    for (uint32_t i = 0; i < ntables; i++) h[i] = tables[i]->desc;
+    cudaError_t e = cudaMalloc(&b->d_tables, sizeof(table_desc) * ntables);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_tables, h, sizeof(table_desc) * ntables, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_scratch, sizeof(unsigned long long) * ((uint64_t)max_ops + 2));
+    free(h);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        pg_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? PG_ERR_NOMEM : PG_ERR_CUDA;
+    }
+    *out = b;
+    return PG_OK;
+}
+
+pg_status pg_batch_destroy(pg_batch *b)
+{
+    if (!b) return PG_ERR_INVALID;
+    cudaFree(b->d_tables);
+    cudaFree(b->d_scratch);
+    free(b);
+    return PG_OK;
+}
+
+pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t lanes_per_key)
+{
+    if (!b) return PG_ERR_INVALID;
+    if (block_threads == 0) block_threads = 256;
+    if (blocks_per_sm == 0) blocks_per_sm = 8;
+    if (lanes_per_key == 0) lanes_per_key = b->lanes;
+    if (b->ifmt == FMT_KV64_FP) lanes_per_key = 1;
+    if (!(lanes_per_key == 1 || lanes_per_key == 2 || lanes_per_key == 4 || lanes_per_key == 8 ||
+          lanes_per_key == 16) ||
+        lanes_per_key > b->bucket)
+        return PG_ERR_UNSUPPORTED;
+    if (block_threads % 32 || block_threads > 256) return PG_ERR_INVALID;
+    b->block_threads = block_threads;
+    b->blocks_per_sm = blocks_per_sm;
+    b->lanes = lanes_per_key;
+    return PG_OK;
+}
+
+pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_nops, const uint64_t *d_keys,
+                       const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
+                       pg_stream_t stream)
+{
+    if (!b || !d_ops || !d_nops || !d_keys) return PG_ERR_INVALID;
+    batch_args a;
+    a.tables = b->d_tables;
+    a.ops = d_ops;
+    a.nops = d_nops;
+    a.chunk_start = b->d_scratch;
+    a.work = b->d_scratch + b->max_ops + 1;
+    a.keys = d_keys;
+    a.vals_in = d_vals_in;
+    a.vals_out = d_vals_out;
+    a.flags = d_flags;
+    a.op_counts = reinterpret_cast<unsigned long long *>(d_op_counts);
+    a.max_ops = b->max_ops;
+    a.ntables = b->ntables;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    k_batch_plan<<<1, 1024, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return PG_ERR_CUDA;
+    dim3 grid((unsigned)(b->num_sms * b->blocks_per_sm)), block(b->block_threads);
+    const int sch = (int)b->scheme;
+    switch (b->ifmt) {
+    case FMT_KV64: e = batch_kv64(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    case FMT_KV64_SPLIT: e = batch_kv64_split(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    case FMT_TAGVAL16: e = batch_tagval16(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    case FMT_TAGVAL16_SPLIT: e = batch_tagval16_split(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    case FMT_KV64_FP: e = batch_kv64_fp(a, b->bucket, 1, sch, b->backing, grid, block, s); break;
+    default: e = batch_tag16(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    }
+    if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;
+    return e == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -10,21 +10,7 @@
 
 using namespace pg;
 
-struct pg_table {
-    pg_table_config cfg;
-    table_desc desc;
-    void *mem[2];
-    uint64_t bytes[2];
-    void *fp;           // fingerprint bytes of level 0 (PG_TABLE_FINGERPRINTS)
-    uint64_t fp_bytes;
-    int device;
-    int num_sms;
-    uint32_t block_threads;
-    uint32_t blocks_per_sm;
-    uint32_t max_blocks;
-    uint32_t lanes;  // lanes per key used by the kernels (defaults to the config's tile)
-    uint32_t ifmt;  // internal format: public format, split variant when PG_TABLE_SPLIT_BUCKETS
-};
+#include "table_internal.h"
 
 namespace {
 
@@ -83,10 +69,7 @@ pg_status cuda_status(cudaError_t e)
     return PG_ERR_CUDA;
 }
 
-uint32_t lanes_of(const pg_table *t)
-{
-    return t->ifmt == FMT_KV64_FP ? 1u : t->lanes;  // the fingerprint walk serves a key with one lane
-}
+uint32_t lanes_of(const pg_table *t) { return pg_table_lanes(t); }
 
 void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block)
 {
@@ -164,6 +147,12 @@ __global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, u
 }
 
 }  // namespace
+
+// lanes a kernel uses per key for this table
+uint32_t pg_table_lanes(const pg_table *t)
+{
+    return t->ifmt == FMT_KV64_FP ? 1u : t->lanes;  // the fingerprint walk serves a key with one lane
+}
 
 extern "C" {
 

@@ -1,0 +1,23 @@
+// table_internal.h -- the table object behind the C ABI's opaque pg_table.
+#pragma once
+#include <stdint.h>
+#include "poggers_b200.h"
+#include "poggers_b200/level.cuh"
+
+struct pg_table {
+    pg_table_config cfg;
+    pg::table_desc desc;
+    void *mem[2];
+    uint64_t bytes[2];
+    void *fp;           // fingerprint bytes of level 0 (PG_TABLE_FINGERPRINTS)
+    uint64_t fp_bytes;
+    int device;
+    int num_sms;
+    uint32_t block_threads;
+    uint32_t blocks_per_sm;
+    uint32_t max_blocks;
+    uint32_t lanes;  // lanes per key used by the kernels (defaults to the config's tile)
+    uint32_t ifmt;  // internal format: public format, split variant when PG_TABLE_SPLIT_BUCKETS
+};
+
+uint32_t pg_table_lanes(const pg_table *t);

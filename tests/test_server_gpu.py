@@ -1,0 +1,127 @@
+"""GPU tests of the continuous-batching server.
+
+Requests are submitted while earlier ones are still on the GPU; each result
+must equal what the same request returns when the requests run one at a time
+in submission order through the plain per-request path (pg_bulk_* on identical
+tables).  uint64 tables: bit-exact (loads stay below the point where inserts
+fail).  Filters: every inserted key found in both runs (placement, hence false
+positives, depends on the order of concurrent inserts in either path)."""
+import numpy as np
+import pytest
+
+from tests.gpu_util import Driver
+from poggers_b200 import workload as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream(rng, ntables, nreq, sizes, kinds):
+    """Seeded request stream: (table, op, keys) with Zipf-ish table choice."""
+    inserted = [[] for _ in range(ntables)]
+    fresh = [0] * ntables
+    reqs = []
+    w = 1.0 / np.arange(1, ntables + 1) ** 0.99
+    w /= w.sum()
+    for _ in range(nreq):
+        t = int(rng.choice(ntables, p=w))
+        n = int(np.exp(rng.uniform(0, np.log(3000))))
+        cap = int(0.6 * sizes[t]) - sum(len(x) for x in inserted[t])
+        u = rng.uniform()
+        if u < 0.3 and cap > n:
+            k = wl.keys_without_sentinels(10_000 * t + 17, fresh[t] + n)[fresh[t]:]
+            fresh[t] += n
+            inserted[t].append(k)
+            reqs.append((t, 0, k))
+        elif u < 0.9 or kinds[t] == "tcf":
+            have = np.concatenate(inserted[t]) if inserted[t] else np.zeros(0, dtype=np.uint64)
+            pos = have[rng.integers(0, len(have), n // 2)] if len(have) else np.zeros(0, dtype=np.uint64)
+            neg = wl.keys_without_sentinels(7_000_000 + rng.integers(1 << 30), n - len(pos))
+            reqs.append((t, 1, np.concatenate([pos, neg])))
+        else:
+            have = np.concatenate(inserted[t]) if inserted[t] else np.zeros(0, dtype=np.uint64)
+            if len(have) == 0:
+                continue
+            reqs.append((t, 2, have[rng.integers(0, len(have), max(1, n // 4))]))
+    return reqs
+
+
+def test_server_results_equal_sequential_plain_path(pg):
+    import torch
+    rng = np.random.default_rng(11)
+    kinds = ["ht"] * 6 + ["ht_fp"] * 3 + ["tcf"] * 5
+    sizes = [int(2 ** rng.uniform(13, 17)) for _ in kinds]
+
+    def cfg(kind, n):
+        if kind == "tcf":
+            return pg.data_structs.tcf(n, max(n // 100, 16))
+        c = pg.data_structs.hash_table_64(n, bucket=8)
+        c.fingerprints = kind == "ht_fp"
+        return c
+
+    srv = pg.Server(hbm_budget_bytes=1 << 34, max_wave_keys=1 << 16, max_wave_requests=256)
+    ids = [srv.add_table(cfg(k, n), 50 + i) for i, (k, n) in enumerate(zip(kinds, sizes))]
+    plain = [pg.Table(cfg(k, n), 50 + i) for i, (k, n) in enumerate(zip(kinds, sizes))]
+    reqs = _stream(rng, len(kinds), 400, sizes, kinds)
+    outs = []
+    rids = []
+    for t, op, keys in reqs:
+        vb = 8 if kinds[t] != "tcf" else 2
+        vals = wl.values_for(keys, vb, 3) if op == 0 else None
+        vout = np.zeros(len(keys), dtype=np.uint64 if vb == 8 else np.uint16)
+        flags = np.zeros(len(keys), dtype=np.uint8)
+        rids.append(srv.submit(ids[t], op, keys, vals, vout, flags))
+        outs.append((vals, vout, flags))
+    res = [srv.poll(r, wait=True) for r in rids]
+    waves, nkeys = srv.stats()
+    assert waves < len(reqs), "requests should share waves"
+    assert nkeys == sum(len(k) for _, _, k in reqs)
+    inserted = [set() for _ in kinds]
+    for (t, op, keys), (vals, vout, flags), (count, lat) in zip(reqs, outs, res):
+        d = Driver(plain[t])
+        f = flags.astype(bool)
+        assert lat >= 0
+        if op == 0:
+            ok = d.insert(keys, vals.astype(np.uint64))
+            if kinds[t] != "tcf":
+                assert (f == ok).all() and f.all()
+            assert count == (~f).sum()
+            inserted[t].update(map(int, keys[f]))
+        elif op == 1:
+            fo, vo = d.query(keys)
+            if kinds[t] == "tcf":
+                known = np.array([int(k) in inserted[t] for k in keys], dtype=bool)
+                assert f[known].all() and fo[known].all()
+            else:
+                assert (f == fo).all() and (vout.astype(np.uint64) == vo).all()
+            assert count == f.sum()
+        else:
+            ro = d.remove(keys)
+            # a request may name a key twice: one of the two removes it, and which
+            # one depends on the order inside the launch, in either path
+            u, inv = np.unique(keys, return_inverse=True)
+            got_s = np.zeros(len(u), dtype=int)
+            got_p = np.zeros(len(u), dtype=int)
+            np.add.at(got_s, inv, f.astype(int))
+            np.add.at(got_p, inv, ro.astype(int))
+            assert (got_s == got_p).all() and got_s.max(initial=0) <= 1
+            assert count == f.sum()
+            for k in keys[f]:
+                inserted[t].discard(int(k))
+    srv.close()
+
+
+def test_server_admits_tables_by_hbm_budget(pg):
+    srv = pg.Server(hbm_budget_bytes=64 << 20, max_wave_keys=1 << 12, max_wave_requests=16)
+    cfg = pg.data_structs.hash_table_64(1 << 20, bucket=8)   # 16 MiB
+    got = [srv.add_table(cfg, i) for i in range(6)]
+    assert got[:4] == [0, 1, 2, 3] and got[4] is None and got[5] is None
+    assert srv.bytes_in_use() == 4 * (16 << 20)
+    srv.drop_table(1)
+    assert srv.add_table(cfg, 9) is not None
+    t = srv.add_table(pg.data_structs.hash_table_64(1 << 10, bucket=8), 3)
+    assert t is None
+    k = wl.keys_without_sentinels(5, 100)
+    f = np.zeros(100, dtype=np.uint8)
+    r = srv.submit(0, 0, k, wl.values_for(k, 8, 1), None, f)
+    assert srv.poll(r, wait=True)[0] == 0 and f.all()
+    srv.close()
