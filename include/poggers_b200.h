@@ -54,7 +54,8 @@ typedef enum pg_status {
     PG_ERR_NOMEM = 3,       /* device allocation failed */
     PG_ERR_UNSUPPORTED = 4, /* valid but not compiled in (bucket size / tile combination) */
     PG_ERR_FULL = 5,        /* capacity exhausted */
-    PG_ERR_TIMEOUT = 6      /* a bounded device wait gave up */
+    PG_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
+    PG_ERR_TOO_LARGE = 7    /* more tables or requests than the fixed scratch of pg_batch_run_static holds */
 } pg_status;
 
 /* slot formats (reference representations) */
@@ -202,6 +203,30 @@ pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t bloc
 pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_nops, const uint64_t *d_keys,
                        const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
                        pg_stream_t stream);
+
+/* Allocation-free variant of pg_batch_run, for callers that cannot call
+ * cudaMalloc (code running inside another allocator, a plugin whose host
+ * forbids device allocations, or a process whose device memory is fully
+ * budgeted).  No counterpart in the reference.  It takes the tables directly
+ * (no pg_batch object) and keeps everything it needs besides the caller's
+ * inputs and outputs -- the tables' device descriptors, the per-request chunk
+ * offsets and the work counter -- in one fixed array compiled into the
+ * library, at most PG_STATIC_MAX_TABLES tables and PG_STATIC_MAX_OPS requests
+ * per call (larger calls return PG_ERR_TOO_LARGE).  That array (about 106 KB)
+ * exists once on every GPU that loads the library, until the process exits.
+ *  - The first call on a device looks up the array's device address; make that
+ *    first call before capturing a stream into a CUDA graph.
+ *  - Every call shares the array and leaves its contents behind (the work
+ *    counter is reset by each call), so calls whose work overlaps on the GPU
+ *    (different streams, or different host threads) race: order them.
+ *  - It allocates no device memory and calls no allocating library routine;
+ *    results equal pg_batch_run's for the same tables and requests. */
+#define PG_STATIC_MAX_TABLES 256
+#define PG_STATIC_MAX_OPS 8192
+pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const pg_op_desc *d_ops,
+                              const uint32_t *d_nops, uint32_t max_ops, const uint64_t *d_keys,
+                              const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
+                              pg_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Continuous-batching server over resident tables (no counterpart in the

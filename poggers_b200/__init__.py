@@ -30,7 +30,9 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("POGGERS_B200_LIB", str(_PKG / "libpoggers_b200.so")))
 
 # ---- enums (include/poggers_b200.h)
-PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT = range(7)
+PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT, PG_ERR_TOO_LARGE = range(8)
+PG_STATIC_MAX_TABLES = 256
+PG_STATIC_MAX_OPS = 8192
 PG_TABLE_SPLIT_BUCKETS = 1
 PG_TABLE_FINGERPRINTS = 2
 FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
@@ -82,7 +84,7 @@ EXPORTED = (
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
-    "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run",
+    "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
 )
@@ -159,6 +161,8 @@ def lib() -> C.CDLL:
     L.pg_batch_set_launch.argtypes = [V, U32, U32, U32]
     L.pg_batch_run.restype = C.c_int
     L.pg_batch_run.argtypes = [V, P, P, P, P, P, P, P, P]
+    L.pg_batch_run_static.restype = C.c_int
+    L.pg_batch_run_static.argtypes = [C.POINTER(V), U32, P, P, U32, P, P, P, P, P, P]
     L.pg_server_create.restype = C.c_int
     L.pg_server_create.argtypes = [C.POINTER(_ServerConfig), C.POINTER(V)]
     L.pg_server_destroy.restype = C.c_int
@@ -556,6 +560,16 @@ class Batch:
         """ops: int64 device tensor from pack_ops; nops: int32 device tensor holding the request count."""
         _check(lib().pg_batch_run(self._h, _ptr(ops), _ptr(nops), _ptr(keys), _ptr(vals_in), _ptr(vals_out),
                                   _ptr(flags), _ptr(op_counts), _stream(stream)), "pg_batch_run")
+
+
+def batch_run_static(tables: list, ops, nops, max_ops: int, keys, vals_in=None, vals_out=None, flags=None,
+                     op_counts=None, stream=None) -> None:
+    """pg_batch_run_static: a batch run that allocates no device memory (its
+    scratch is a fixed array inside the library; see include/poggers_b200.h)."""
+    arr = (C.c_void_p * len(tables))(*[t.handle.value for t in tables])
+    _check(lib().pg_batch_run_static(arr, len(tables), _ptr(ops), _ptr(nops), max_ops, _ptr(keys), _ptr(vals_in),
+                                     _ptr(vals_out), _ptr(flags), _ptr(op_counts), _stream(stream)),
+           "pg_batch_run_static")
 
 
 # ---------------------------------------------------------------- serving

@@ -4,6 +4,8 @@
 #include <string.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "poggers_b200.h"
 #include "batch_kernels.cuh"
 #include "table_internal.h"
@@ -66,6 +68,50 @@ __global__ void __launch_bounds__(1024) k_batch_plan(batch_args a)
 }
 
 }  // namespace pg
+
+namespace {
+
+// ---- scratch of pg_batch_run_static -------------------------------------
+// For callers that cannot allocate device memory (code running where
+// cudaMalloc is not available to it, e.g. inside another allocator, a
+// driver-level plugin or an environment whose memory is fully budgeted), the
+// batch run can use this fixed array instead of pg_batch_create's buffers.
+// Every GPU that loads the library holds one copy until the process exits.
+constexpr uint32_t kStaticMaxTables = PG_STATIC_MAX_TABLES;
+constexpr uint32_t kStaticMaxOps = PG_STATIC_MAX_OPS;
+
+struct static_scratch {
+    table_desc tables[kStaticMaxTables];
+    unsigned long long chunk_start[kStaticMaxOps + 1];
+    unsigned long long work;
+};
+
+static __device__ __align__(256) unsigned char g_batch_static[sizeof(static_scratch)];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void *g_static_addr[kMaxDevices];      // device address of g_batch_static, per device
+table_desc g_static_stage[kStaticMaxTables];  // host staging of the descriptors (guarded by g_static_mu)
+
+// The symbol's device address on the current device; the first call on each
+// device looks it up (cudaGetSymbolAddress, with that device current).
+pg_status static_scratch_addr(static_scratch **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PG_ERR_CUDA;
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_batch_static) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return PG_ERR_CUDA;
+        }
+        g_static_addr[dev] = p;
+    }
+    *out = static_cast<static_scratch *>(g_static_addr[dev]);
+    return PG_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -168,6 +214,65 @@ pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_n
     case FMT_TAGVAL16_SPLIT: e = batch_tagval16_split(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
     case FMT_KV64_FP: e = batch_kv64_fp(a, b->bucket, 1, sch, b->backing, grid, block, s); break;
     default: e = batch_tag16(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
+    }
+    if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;
+    return e == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
+
+pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const pg_op_desc *d_ops,
+                              const uint32_t *d_nops, uint32_t max_ops, const uint64_t *d_keys,
+                              const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
+                              pg_stream_t stream)
+{
+    if (!tables || ntables == 0 || !d_ops || !d_nops || !d_keys || max_ops == 0) return PG_ERR_INVALID;
+    if (ntables > kStaticMaxTables || max_ops > kStaticMaxOps) return PG_ERR_TOO_LARGE;
+    const pg_table *t0 = tables[0];
+    if (!t0) return PG_ERR_INVALID;
+    for (uint32_t i = 1; i < ntables; i++) {
+        const pg_table *t = tables[i];
+        if (!t || t->ifmt != t0->ifmt || t->cfg.levels[0].bucket_size != t0->cfg.levels[0].bucket_size ||
+            t->cfg.levels[0].scheme != t0->cfg.levels[0].scheme || (t->cfg.nlevels > 1) != (t0->cfg.nlevels > 1) ||
+            t->device != t0->device)
+            return PG_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> g(g_static_mu);
+    static_scratch *sc = nullptr;
+    pg_status st = static_scratch_addr(&sc);
+    if (st != PG_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // the descriptors go through a fixed host array; a copy from pageable
+    // memory returns once the source has been read, so the array can be reused
+    for (uint32_t i = 0; i < ntables; i++) g_static_stage[i] = tables[i]->desc;
+    if (cudaMemcpyAsync(sc->tables, g_static_stage, sizeof(table_desc) * ntables, cudaMemcpyHostToDevice, s) !=
+        cudaSuccess)
+        return PG_ERR_CUDA;
+    batch_args a;
+    a.tables = sc->tables;
+    a.ops = d_ops;
+    a.nops = d_nops;
+    a.chunk_start = sc->chunk_start;
+    a.work = &sc->work;  // zeroed by k_batch_plan on every call
+    a.keys = d_keys;
+    a.vals_in = d_vals_in;
+    a.vals_out = d_vals_out;
+    a.flags = d_flags;
+    a.op_counts = reinterpret_cast<unsigned long long *>(d_op_counts);
+    a.max_ops = max_ops;
+    a.ntables = ntables;
+    k_batch_plan<<<1, 1024, 0, s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return PG_ERR_CUDA;
+    dim3 grid((unsigned)(t0->num_sms * 8)), block(256);
+    const uint32_t lanes = pg_table_lanes(t0), bucket = t0->cfg.levels[0].bucket_size;
+    const int sch = (int)t0->cfg.levels[0].scheme;
+    const bool bk = t0->cfg.nlevels > 1;
+    cudaError_t e;
+    switch (t0->ifmt) {
+    case FMT_KV64: e = batch_kv64(a, bucket, lanes, sch, bk, grid, block, s); break;
+    case FMT_KV64_SPLIT: e = batch_kv64_split(a, bucket, lanes, sch, bk, grid, block, s); break;
+    case FMT_TAGVAL16: e = batch_tagval16(a, bucket, lanes, sch, bk, grid, block, s); break;
+    case FMT_TAGVAL16_SPLIT: e = batch_tagval16_split(a, bucket, lanes, sch, bk, grid, block, s); break;
+    case FMT_KV64_FP: e = batch_kv64_fp(a, bucket, 1, sch, bk, grid, block, s); break;
+    default: e = batch_tag16(a, bucket, lanes, sch, bk, grid, block, s); break;
     }
     if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;
     return e == cudaSuccess ? PG_OK : PG_ERR_CUDA;

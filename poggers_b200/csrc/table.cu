@@ -168,6 +168,9 @@ const char *pg_status_string(pg_status s)
     case PG_ERR_UNSUPPORTED: return "unsupported configuration";
     case PG_ERR_FULL: return "capacity exhausted";
     case PG_ERR_TIMEOUT: return "bounded device wait timed out";
+    case PG_ERR_TOO_LARGE:
+        return "more tables or requests than pg_batch_run_static's fixed scratch holds "
+               "(PG_STATIC_MAX_TABLES / PG_STATIC_MAX_OPS)";
     }
     return "unknown status";
 }
