@@ -147,6 +147,7 @@ def run_ours(args, rank, world):
     cfg.fingerprints = args.layout == "fingerprints"
     table = pg.Table(cfg, SEED)
     table.set_launch(BLOCK_THREADS, BLOCKS_PER_SM, 0, LANES)
+    table.set_partitioned_insert(args.insert_order == "region")
     stream = torch.cuda.current_stream()
 
     def step(ev=None):
@@ -202,6 +203,10 @@ def run_ours(args, rank, world):
 
     e2e = None if args.no_e2e else run_e2e(args, table, keys, vals, qkeys, dev, world)
 
+    # per step: the insert kernel (after the region count, scan and scatter kernels
+    # when the batch is region-ordered) and the query kernel; clears are memsets
+    ordered = args.insert_order == "region" and n >= (1 << 20) and NSLOTS * 16 >= (64 << 20)
+    launches_per_step = (4 if ordered else 1) + 1
     ops = (n + nq) * args.steps * world
     value = ops / (ms_max / 1e3) / 1e6
     peak, peak_kind = peaks()
@@ -220,7 +225,7 @@ def run_ours(args, rank, world):
         "config": {"workload": WORKLOAD, "slots": NSLOTS, "inserts": n, "queries": nq,
                    "launch": {"lanes_per_key": 1 if args.layout == "fingerprints" else LANES,
                               "block_threads": BLOCK_THREADS, "blocks_per_sm": BLOCKS_PER_SM,
-                              "bucket_layout": args.layout},
+                              "bucket_layout": args.layout, "insert_order": args.insert_order},
                    "parallelism": f"independent table per GPU x{world}",
                    "l2": "inputs larger than L2 (1 GiB table, 126 MB L2)"},
         "roofline": {"bound": "hbm", "kernel": f"bulk_{dom}", "achieved": round(achieved, 1),
@@ -230,7 +235,7 @@ def run_ours(args, rank, world):
                     "insert_mops": round(n / ins_ms / 1e3, 1), "query_mops": round(nq / qry_ms / 1e3, 1),
                     "remove_mops": round(len(rem) / rem_ms / 1e3, 1),
                     "insert_failures": int((~okn).sum())},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "e2e": e2e,
     }
@@ -454,6 +459,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--layout", choices=["fingerprints", "interleaved", "split"], default=LAYOUT)
+    ap.add_argument("--insert-order", choices=["region", "batch"], default="region",
+                    help="region: inserts counting-sorted by table region (default); batch: in batch order")
     ap.add_argument("--slots-log2", type=int, default=26,
                     help="table size (default 26 = the benchmark workload; smaller only for profiling captures)")
     args = ap.parse_args()

@@ -143,8 +143,22 @@ uint64_t pg_table_bytes(const pg_table *t);
 pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
                               uint32_t lanes_per_key);
 
+/* Region-ordered inserts (on by default; enable = 0 turns them off).  A
+ * batch of at least 2^20 keys into a uint64 bucket table of at least 64 MB
+ * is first counting-sorted by the table region (32 MB) of each key's first
+ * bucket, then inserted in that order, so each bucket line is fetched from
+ * HBM once for all its keys instead of once per key.  The sort costs 20
+ * bytes of device scratch per key, allocated by the first such insert and
+ * kept by the table (counted in pg_table_bytes) until pg_table_destroy.
+ * Concurrent inserts have no defined order in the reference either: which
+ * keys fail when a table overflows may differ, every placed key is
+ * placed by the same rule. */
+pg_status pg_table_set_partitioned_insert(pg_table *t, int enable);
+
 /* Bulk insert of n keys (and values; d_vals may be NULL = all 0).
- * d_ok[i] (optional) = 1 if key i was placed; d_fail_count (optional) += failures. */
+ * d_ok[i] (optional) = 1 if key i was placed; d_fail_count (optional) += failures.
+ * Replaces the reference's per-tile insert loop over a batch
+ * (tables/base_table.cuh:174-214, driven one key per tile by its tests). */
 pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
                          uint8_t *d_ok, uint64_t *d_fail_count, pg_stream_t stream);
 

@@ -78,7 +78,8 @@ _lib = None
 
 EXPORTED = (
     "pg_version", "pg_status_string", "pg_table_create", "pg_table_destroy", "pg_table_clear",
-    "pg_table_level_info", "pg_table_bytes", "pg_table_set_launch", "pg_bulk_insert", "pg_bulk_query",
+    "pg_table_level_info", "pg_table_bytes", "pg_table_set_launch", "pg_table_set_partitioned_insert",
+    "pg_bulk_insert", "pg_bulk_query",
     "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
@@ -115,6 +116,8 @@ def lib() -> C.CDLL:
     L.pg_table_bytes.argtypes = [V]
     L.pg_table_set_launch.restype = C.c_int
     L.pg_table_set_launch.argtypes = [V, U32, U32, U32, U32]
+    L.pg_table_set_partitioned_insert.restype = C.c_int
+    L.pg_table_set_partitioned_insert.argtypes = [V, C.c_int]
     L.pg_bulk_insert.restype = C.c_int
     L.pg_bulk_insert.argtypes = [V, P, P, U64, P, P, P]
     L.pg_bulk_query.restype = C.c_int
@@ -310,6 +313,10 @@ class Table:
                    lanes_per_key: int = 0) -> None:
         _check(lib().pg_table_set_launch(self._h, block_threads, blocks_per_sm, max_blocks, lanes_per_key),
                "pg_table_set_launch")
+
+    def set_partitioned_insert(self, enable: bool) -> None:
+        """Region-ordered inserts for large batches (on by default)."""
+        _check(lib().pg_table_set_partitioned_insert(self._h, int(bool(enable))), "pg_table_set_partitioned_insert")
 
     def serial(self, lanes_per_key: int = 0) -> None:
         """One group walks the batch in order (deterministic layout, for parity checks)."""

@@ -21,6 +21,9 @@ struct bulk_args {
     uint8_t *flags;                 // ok / found
     unsigned long long *count;      // fail count (insert) or hit count (query / remove)
     uint64_t n;
+    // insert over a permuted copy of the batch: flags were preset to 1 and only
+    // a failure is written, at flags[perm[i]] (the key's place in the caller's batch)
+    const uint32_t *perm;
 };
 
 __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
@@ -56,7 +59,10 @@ __global__ void __launch_bounds__(256, PG_MIN_BLOCKS) k_bulk(table_desc t, bulk_
             V v = vin ? __ldg(vin + i) : (V)0;
             r = T::insert(t, g, key, v);
             if (g.gl == 0) {
-                if (a.flags) __stcs(a.flags + i, (uint8_t)r);
+                if (a.flags) {
+                    if (!a.perm) __stcs(a.flags + i, (uint8_t)r);
+                    else if (!r) a.flags[a.perm[i]] = 0;
+                }
                 c += !r;
             }
         } else if constexpr (OP == OP_QUERY) {

@@ -1,0 +1,224 @@
+// partition.cu -- region-ordered bulk insert for large batches into large
+// uint64 tables.
+//
+// A random insert into a table much larger than L2 costs a DRAM read for its
+// CAS and a DRAM write-back of the dirty sector, per key: random DRAM
+// transactions are the limit.  Sorting the batch by the table region of each
+// key's first bucket (a counting sort into R regions that each fit in L2) lets
+// the insert kernel sweep the table region by region: while the resident
+// threads work through one region, its lines stay in L2, so a line is
+// fetched once and written back once for all the keys that land in it (about
+// seven at 0.9 load with 8-slot buckets) instead of once per key.  Keys whose
+// first bucket is full still probe at random.
+//
+// The per-key work is the ordinary insert; only the order in which a launch
+// visits the keys changes, and concurrent inserts have no defined order in
+// the reference either.  The caller's ok flags are preset to 1 and a failed
+// insert clears its flag through the permutation.
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#include "poggers_b200.h"
+#include "bulk_kernels.cuh"
+#include "table_internal.h"
+
+namespace pg {
+
+constexpr uint32_t kPartThreads = 256;
+constexpr uint32_t kPartPerThread = 4;
+constexpr uint32_t kPartTile = kPartThreads * kPartPerThread;  // keys per scatter tile
+constexpr uint32_t kPartMaxRegions = 1024;
+#ifndef PG_PART_REGION_MB
+#define PG_PART_REGION_MB 32
+#endif
+constexpr uint64_t kPartRegionBytes = (uint64_t)PG_PART_REGION_MB << 20;  // table bytes per region (a power of two)
+constexpr uint64_t kPartMinKeys = 1ull << 20;         // smaller batches insert unsorted
+
+// region of a key = its first bucket >> shift: regions are runs of 2^shift buckets
+__device__ __forceinline__ uint32_t region_of(const level_desc &L, uint64_t key, uint32_t shift)
+{
+    return (uint32_t)(L.nbmod.mod(murmur64a_u64(key, L.seed)) >> shift);
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_part_count(level_desc L, const uint64_t *keys, uint64_t n,
+                                                             uint32_t shift, uint32_t R, unsigned long long *counts)
+{
+    __shared__ unsigned int hist[kPartMaxRegions];
+    for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) hist[r] = 0;
+    __syncthreads();
+    // kPartPerThread keys per thread per round, all loads issued before any is used
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * kPartPerThread) {
+        uint64_t k[kPartPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerThread; j++) {
+            const uint64_t i = i0 + j * stride;
+            k[j] = i < n ? __ldcs(keys + i) : 0;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerThread; j++)
+            if (i0 + j * stride < n) atomicAdd(&hist[region_of(L, k[j], shift)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < R; r += blockDim.x)
+        if (hist[r]) atomicAdd(counts + r, (unsigned long long)hist[r]);
+}
+
+// exclusive prefix sum of the R region counts into the cursors (one warp)
+__global__ void k_part_scan(const unsigned long long *counts, unsigned long long *cursors, uint32_t R)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long carry = 0;
+    for (uint32_t r0 = 0; r0 < R; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        const unsigned long long c = r < R ? counts[r] : 0ULL;
+        unsigned long long x = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= (uint32_t)d) x += y;
+        }
+        if (r < R) cursors[r] = carry + x - c;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
+// One tile of kPartTile keys at a time: count the tile's keys per region in
+// shared memory, reserve one run per region from the global cursors, sort the
+// tile by region in shared memory, then write each region's run with
+// consecutive threads on consecutive addresses.
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter(level_desc L, const uint64_t *keys,
+                                                               const unsigned long long *vals, uint64_t n,
+                                                               uint32_t shift, uint32_t R,
+                                                               unsigned long long *cursors, uint64_t *okeys,
+                                                               unsigned long long *ovals, uint32_t *operm)
+{
+    __shared__ unsigned long long gbase[kPartMaxRegions];
+    __shared__ unsigned int cnt[kPartMaxRegions];
+    __shared__ unsigned int lstart[kPartMaxRegions];
+    __shared__ uint64_t sk[kPartTile];
+    __shared__ unsigned long long sv[kPartTile];
+    __shared__ uint32_t sp[kPartTile];
+    __shared__ uint16_t sr[kPartTile];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    for (uint64_t t0 = (uint64_t)blockIdx.x * kPartTile; t0 < n; t0 += (uint64_t)gridDim.x * kPartTile) {
+        const uint32_t tn = (uint32_t)((n - t0) < kPartTile ? (n - t0) : kPartTile);
+        for (uint32_t r = tid; r < R; r += blockDim.x) cnt[r] = 0;
+        __syncthreads();
+        uint64_t k[kPartPerThread];
+        unsigned long long v[kPartPerThread];
+        uint32_t reg[kPartPerThread], rank[kPartPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerThread; j++) {
+            const uint32_t e = j * kPartThreads + tid;
+            if (e < tn) {
+                k[j] = __ldcs(keys + t0 + e);
+                v[j] = ovals ? __ldcs(vals + t0 + e) : 0ULL;
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerThread; j++) {
+            const uint32_t e = j * kPartThreads + tid;
+            reg[j] = 0xFFFFFFFFu;
+            if (e < tn) {
+                reg[j] = region_of(L, k[j], shift);
+                rank[j] = atomicAdd(&cnt[reg[j]], 1u);
+            }
+        }
+        __syncthreads();
+        // tile-local exclusive scan of cnt (warp 0) and the global reservations (all threads)
+        if (warp == 0) {
+            unsigned int carry = 0;
+            for (uint32_t r0 = 0; r0 < R; r0 += 32) {
+                const uint32_t r = r0 + lane;
+                const unsigned int c = r < R ? cnt[r] : 0u;
+                unsigned int x = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const unsigned int y = __shfl_up_sync(0xffffffffu, x, d);
+                    if (lane >= (uint32_t)d) x += y;
+                }
+                if (r < R) lstart[r] = carry + x - c;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+        }
+        for (uint32_t r = tid; r < R; r += blockDim.x)
+            if (cnt[r]) gbase[r] = atomicAdd(cursors + r, (unsigned long long)cnt[r]);
+        __syncthreads();
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerThread; j++) {
+            if (reg[j] == 0xFFFFFFFFu) continue;
+            const uint32_t e = j * kPartThreads + tid;
+            const uint32_t at = lstart[reg[j]] + rank[j];
+            sk[at] = k[j];
+            sv[at] = v[j];
+            sp[at] = (uint32_t)(t0 + e);
+            sr[at] = (uint16_t)reg[j];
+        }
+        __syncthreads();
+        for (uint32_t e = tid; e < tn; e += blockDim.x) {
+            const uint32_t r = sr[e];
+            const uint64_t pos = gbase[r] + (e - lstart[r]);
+            okeys[pos] = sk[e];
+            if (ovals) ovals[pos] = sv[e];
+            operm[pos] = sp[e];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+// Called by pg_bulk_insert with the caller's batch in `a`.  When the batch
+// qualifies it writes the region-ordered copy into the table's scratch,
+// presets the ok flags to 1, points `a` at the copy and returns true; the
+// caller then runs the ordinary insert launch on `a`.  Returns false (and
+// leaves `a` alone) when the batch should take the ordinary path: partitioning
+// off, a serial launch shape, not a uint64 bucket table, table or batch too
+// small for the sort to pay, or no memory for the scratch.
+bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
+{
+    const uint64_t n = a.n;
+    const bool kv64 = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT || t->ifmt == FMT_KV64_FP;
+    if (!t->partition || !kv64 || t->cfg.levels[0].scheme != PG_SCHEME_BUCKET || t->max_blocks == 1) return false;
+    if (t->bytes[0] < 2 * kPartRegionBytes || n < kPartMinKeys || n >= (1ull << 32)) return false;
+    // regions of 2^shift buckets, about kPartRegionBytes of slots each, at most kPartMaxRegions
+    const uint64_t nb = t->desc.lv[0].nbmod.d, bucket_bytes = t->bytes[0] / nb;
+    uint32_t shift = 0;
+    while ((bucket_bytes << (shift + 1)) <= kPartRegionBytes) shift++;
+    while (((nb - 1) >> shift) + 1 > kPartMaxRegions) shift++;
+    const uint32_t R = (uint32_t)(((nb - 1) >> shift) + 1);
+    // scratch: keys (8 B), values (8 B), original index (4 B) per key; counts and cursors per region
+    const uint64_t cnt_off = (n * 20 + 255) & ~255ull;
+    const uint64_t need = cnt_off + 2ull * R * 8;
+    if (t->part_bytes < need) {
+        if (t->part_buf) cudaFree(t->part_buf);
+        t->part_buf = nullptr;
+        t->part_bytes = 0;
+        if (cudaMalloc(&t->part_buf, need) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        t->part_bytes = need;
+    }
+    unsigned char *p = static_cast<unsigned char *>(t->part_buf);
+    uint64_t *okeys = reinterpret_cast<uint64_t *>(p);
+    unsigned long long *ovals = a.vals_in ? reinterpret_cast<unsigned long long *>(p + n * 8) : nullptr;
+    uint32_t *operm = reinterpret_cast<uint32_t *>(p + n * 16);
+    unsigned long long *counts = reinterpret_cast<unsigned long long *>(p + cnt_off);
+    unsigned long long *cursors = counts + R;
+    const level_desc &L = t->desc.lv[0];
+    const unsigned grid = (unsigned)(t->num_sms * 8);
+    cudaMemsetAsync(counts, 0, R * 8, s);
+    k_part_count<<<grid, kPartThreads, 0, s>>>(L, a.keys, n, shift, R, counts);
+    k_part_scan<<<1, 32, 0, s>>>(counts, cursors, R);
+    k_part_scatter<<<grid, kPartThreads, 0, s>>>(L, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
+                                                 shift, R, cursors, okeys, ovals, operm);
+    if (a.flags) cudaMemsetAsync(a.flags, 1, n, s);
+    a.keys = okeys;
+    a.vals_in = ovals;
+    a.perm = operm;
+    return true;
+}

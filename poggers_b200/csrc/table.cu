@@ -71,12 +71,14 @@ pg_status cuda_status(cudaError_t e)
 
 uint32_t lanes_of(const pg_table *t) { return pg_table_lanes(t); }
 
-void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block)
+// ordered: one group per key with no wrap-around (a region-ordered batch), so
+// the resident blocks always cover one contiguous window of the batch
+void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block, bool ordered = false)
 {
     const uint32_t bt = t->block_threads;
     const uint64_t groups_per_block = bt / lanes_of(t);
     uint64_t need = (n + groups_per_block - 1) / groups_per_block;
-    uint64_t cap = (uint64_t)t->num_sms * t->blocks_per_sm;
+    uint64_t cap = ordered ? 0x7fffffffull : (uint64_t)t->num_sms * t->blocks_per_sm;
     if (t->max_blocks && cap > t->max_blocks) cap = t->max_blocks;
     if (need > cap) need = cap;
     if (need == 0) need = 1;
@@ -90,17 +92,18 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     if (a.n == 0) return PG_OK;
     if (!a.keys) return PG_ERR_INVALID;
     dim3 grid, block;
-    launch_shape(t, a.n, grid, block);
+    launch_shape(t, a.n, grid, block, a.perm != nullptr);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t b0 = t->cfg.levels[0].bucket_size, tile = lanes_of(t);
+    const table_desc &d = t->desc;
     cudaError_t e;
     switch (t->ifmt) {
-    case FMT_KV64: e = launch_kv64(op, b0, tile, t->desc, a, grid, block, s); break;
-    case FMT_KV64_SPLIT: e = launch_kv64_split(op, b0, tile, t->desc, a, grid, block, s); break;
-    case FMT_TAGVAL16: e = launch_tagval16(op, b0, tile, t->desc, a, grid, block, s); break;
-    case FMT_TAGVAL16_SPLIT: e = launch_tagval16_split(op, b0, tile, t->desc, a, grid, block, s); break;
-    case FMT_KV64_FP: e = launch_kv64_fp(op, b0, tile, t->desc, a, grid, block, s); break;
-    default: e = launch_tag16(op, b0, tile, t->desc, a, grid, block, s); break;
+    case FMT_KV64: e = launch_kv64(op, b0, tile, d, a, grid, block, s); break;
+    case FMT_KV64_SPLIT: e = launch_kv64_split(op, b0, tile, d, a, grid, block, s); break;
+    case FMT_TAGVAL16: e = launch_tagval16(op, b0, tile, d, a, grid, block, s); break;
+    case FMT_TAGVAL16_SPLIT: e = launch_tagval16_split(op, b0, tile, d, a, grid, block, s); break;
+    case FMT_KV64_FP: e = launch_kv64_fp(op, b0, tile, d, a, grid, block, s); break;
+    default: e = launch_tag16(op, b0, tile, d, a, grid, block, s); break;
     }
     return cuda_status(e);
 }
@@ -193,6 +196,7 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
     t->blocks_per_sm = 32;
     t->max_blocks = 0;
     t->lanes = cfg->tile;
+    t->partition = 1;
     t->ifmt = internal_format(cfg);
     t->desc.nlevels = cfg->nlevels;
     t->desc.format = t->ifmt;
@@ -246,6 +250,7 @@ pg_status pg_table_destroy(pg_table *t)
     for (int l = 0; l < 2; l++)
         if (t->mem[l] && cudaFree(t->mem[l]) != cudaSuccess) st = PG_ERR_CUDA;
     if (t->fp && cudaFree(t->fp) != cudaSuccess) st = PG_ERR_CUDA;
+    if (t->part_buf && cudaFree(t->part_buf) != cudaSuccess) st = PG_ERR_CUDA;
     free(t);
     return st;
 }
@@ -276,7 +281,14 @@ pg_status pg_table_level_info(const pg_table *t, uint32_t level, pg_level_info *
 uint64_t pg_table_bytes(const pg_table *t)
 {
     if (!t) return 0;
-    return t->bytes[0] + t->bytes[1] + t->fp_bytes;
+    return t->bytes[0] + t->bytes[1] + t->fp_bytes + t->part_bytes;
+}
+
+pg_status pg_table_set_partitioned_insert(pg_table *t, int enable)
+{
+    if (!t) return PG_ERR_INVALID;
+    t->partition = enable != 0;
+    return PG_OK;
 }
 
 pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
@@ -304,6 +316,7 @@ pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals
 {
     bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
                 reinterpret_cast<unsigned long long *>(d_fail_count), n};
+    if (t && d_keys && n) pg_partition_insert(t, a, reinterpret_cast<cudaStream_t>(stream));
     return run_bulk(t, OP_INSERT, a, stream);
 }
 

@@ -3,6 +3,7 @@
 #include <stdint.h>
 #include "poggers_b200.h"
 #include "poggers_b200/level.cuh"
+#include <cuda_runtime.h>
 
 struct pg_table {
     pg_table_config cfg;
@@ -18,6 +19,13 @@ struct pg_table {
     uint32_t max_blocks;
     uint32_t lanes;  // lanes per key used by the kernels (defaults to the config's tile)
     uint32_t ifmt;  // internal format: public format, split variant when PG_TABLE_SPLIT_BUCKETS
+    uint32_t partition;  // region-ordered inserts enabled
+    void *part_buf;      // their scratch (keys, values, original index, region counts)
+    uint64_t part_bytes;
 };
 
 uint32_t pg_table_lanes(const pg_table *t);
+
+namespace pg { struct bulk_args; }
+// Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted copy.
+bool pg_partition_insert(pg_table *t, pg::bulk_args &a, cudaStream_t s);
