@@ -37,7 +37,9 @@ enum {
 /* insert schemes */
 enum {
     PGO_SCHEME_BUCKET = 0,     /* insert_schemes/bucket_insert.cuh */
-    PGO_SCHEME_TWO_CHOICE = 1  /* insert_schemes/power_of_n_shortcut.cuh */
+    PGO_SCHEME_TWO_CHOICE = 1, /* insert_schemes/power_of_n_shortcut.cuh */
+    PGO_SCHEME_TWO_CHOICE_BUCKETED = 2, /* insert_schemes/power_of_n_shortcut_buckets.cuh */
+    PGO_SCHEME_LINEAR_BUCKETED = 3      /* insert_schemes/linear_insert_buckets.cuh */
 };
 
 /* probing schemes */
@@ -114,6 +116,38 @@ uint64_t pgo_slab_capacity(const pgo_slab *s);
 uint64_t pgo_slab_free_objects(const pgo_slab *s);
 uint64_t pgo_slab_malloc(pgo_slab *s, uint64_t n, uint64_t *offsets);
 uint64_t pgo_slab_free(pgo_slab *s, uint64_t n, const uint64_t *offsets);
+
+/* Bucketed two-choice filter with tombstone reuse (tables/bucketed_table.cuh
+ * over packed_bucket + grouped_bits_pair slots): poggers_oracle_bucketed.c.
+ * tag_bits 16: 4-byte slots (16-bit tag, 16-bit value), tag_bits 8: 2-byte
+ * slots.  Levels use PGO_SCHEME_TWO_CHOICE_BUCKETED or PGO_SCHEME_LINEAR_BUCKETED. */
+enum {
+    PGO_BOP_INSERT = 0,
+    PGO_BOP_QUERY = 1,
+    PGO_BOP_REMOVE = 2,
+    PGO_BOP_INSERT_DELETE = 3,               /* insert_with_delete */
+    PGO_BOP_INSERT_IF_NOT_EXISTS = 4,
+    PGO_BOP_INSERT_IF_NOT_EXISTS_DELETE = 5
+};
+typedef struct pgo_bcfg {
+    uint32_t tag_bits;
+    uint32_t nlevels;
+    uint32_t pad0, pad1;
+    pgo_level_cfg lv[2];
+} pgo_bcfg;
+typedef struct pgo_btable pgo_btable;
+uint64_t pgo_btag(uint32_t bits, uint64_t key);
+pgo_btable *pgo_btable_create(const pgo_bcfg *cfg, uint64_t seed);
+void pgo_btable_destroy(pgo_btable *t);
+uint64_t pgo_btable_level_bytes(const pgo_btable *t, int level);
+uint64_t pgo_btable_level_nbuckets(const pgo_btable *t, int level);
+void *pgo_btable_level_data(pgo_btable *t, int level);
+/* one operation; *out = value found (query / insert_if_not_exists*), *found = found_val */
+int pgo_btable_op(pgo_btable *t, int op, uint64_t key, uint64_t val, uint64_t *out, int *found);
+/* sequential bulk form in batch order; returns how many calls returned true */
+uint64_t pgo_btable_bulk(pgo_btable *t, int op, const uint64_t *keys, const uint64_t *vals, uint64_t n,
+                         uint64_t *out, uint8_t *ok, uint8_t *found);
+uint64_t pgo_btable_count_fill(const pgo_btable *t, int level);
 
 /* splitmix64 key stream: key i = mix(seed + (i+1) * 0x9E3779B97F4A7C15) */
 void pgo_splitmix64_fill(uint64_t seed, uint64_t start, uint64_t n, uint64_t *out);

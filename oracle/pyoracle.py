@@ -19,7 +19,8 @@ REFHOST_PATH = HERE / "_ref" / "libpoggers_refhost.so"
 REFCUDA_PATH = HERE / "_ref" / "libpoggers_refcuda.so"
 
 FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
-SCHEME_BUCKET, SCHEME_TWO_CHOICE = 0, 1
+SCHEME_BUCKET, SCHEME_TWO_CHOICE, SCHEME_TWO_CHOICE_BUCKETED, SCHEME_LINEAR_BUCKETED = 0, 1, 2, 3
+BOP_INSERT, BOP_QUERY, BOP_REMOVE, BOP_INSERT_DELETE, BOP_INSERT_IF_NOT_EXISTS, BOP_INSERT_IF_NOT_EXISTS_DELETE = range(6)
 PROBE_DOUBLE, PROBE_LINEAR, PROBE_P2, PROBE_XOR_P2 = 0, 1, 2, 3
 SLOT_BYTES = {FMT_KV64: 16, FMT_TAGVAL16: 4, FMT_TAG16: 2}
 
@@ -27,6 +28,11 @@ SLOT_BYTES = {FMT_KV64: 16, FMT_TAGVAL16: 4, FMT_TAG16: 2}
 class LevelCfg(C.Structure):
     _fields_ = [("nslots", C.c_uint64), ("bucket_size", C.c_uint32), ("max_probes", C.c_uint32),
                 ("scheme", C.c_uint32), ("probe", C.c_uint32)]
+
+
+class BCfg(C.Structure):
+    _fields_ = [("tag_bits", C.c_uint32), ("nlevels", C.c_uint32), ("pad0", C.c_uint32), ("pad1", C.c_uint32),
+                ("lv", LevelCfg * 2)]
 
 
 class Cfg(C.Structure):
@@ -99,6 +105,22 @@ def lib():
         L.pgo_slab_malloc.argtypes = [C.c_void_p, C.c_uint64, U64P]
         L.pgo_slab_free.restype = C.c_uint64
         L.pgo_slab_free.argtypes = [C.c_void_p, C.c_uint64, U64P]
+        L.pgo_btag.restype = C.c_uint64
+        L.pgo_btag.argtypes = [C.c_uint32, C.c_uint64]
+        L.pgo_btable_create.restype = C.c_void_p
+        L.pgo_btable_create.argtypes = [C.POINTER(BCfg), C.c_uint64]
+        L.pgo_btable_destroy.argtypes = [C.c_void_p]
+        for f in ("pgo_btable_level_bytes", "pgo_btable_level_nbuckets"):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_void_p, C.c_int]
+        L.pgo_btable_level_data.restype = C.c_void_p
+        L.pgo_btable_level_data.argtypes = [C.c_void_p, C.c_int]
+        L.pgo_btable_op.restype = C.c_int
+        L.pgo_btable_op.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint64, U64P, C.POINTER(C.c_int)]
+        L.pgo_btable_bulk.restype = C.c_uint64
+        L.pgo_btable_bulk.argtypes = [C.c_void_p, C.c_int, U64P, U64P, C.c_uint64, U64P, U8P, U8P]
+        L.pgo_btable_count_fill.restype = C.c_uint64
+        L.pgo_btable_count_fill.argtypes = [C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -244,3 +266,44 @@ class OracleSlab:
     def free(self, offsets) -> int:
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         return lib().pgo_slab_free(self.h, len(offsets), _p64(offsets))
+
+
+class OracleBucketed:
+    """Sequential model of the reference's bucketed_table with packed slots
+    (del_TCF: tag_bits 16; del_TCF_small: tag_bits 8).
+    levels: [(nslots, bucket_size, max_probes, scheme, probe), ...]"""
+
+    def __init__(self, tag_bits: int, levels: list[tuple], seed: int):
+        c = BCfg()
+        c.tag_bits, c.nlevels = tag_bits, len(levels)
+        for i, lv in enumerate(levels):
+            c.lv[i] = LevelCfg(*lv)
+        self.cfg = c
+        self.h = lib().pgo_btable_create(C.byref(c), seed)
+        if not self.h:
+            raise ValueError("invalid bucketed oracle configuration")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pgo_btable_destroy(self.h)
+            self.h = None
+
+    def level_bytes(self, level: int) -> bytes:
+        n = lib().pgo_btable_level_bytes(self.h, level)
+        return C.string_at(lib().pgo_btable_level_data(self.h, level), n)
+
+    def nbuckets(self, level: int) -> int:
+        return lib().pgo_btable_level_nbuckets(self.h, level)
+
+    def bulk(self, op: int, keys, vals=None):
+        """(ok, out values, found) after running `op` on every key in batch order."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        vals = None if vals is None else np.ascontiguousarray(vals, dtype=np.uint64)
+        out = np.zeros(len(keys), dtype=np.uint64)
+        ok = np.zeros(len(keys), dtype=np.uint8)
+        found = np.zeros(len(keys), dtype=np.uint8)
+        lib().pgo_btable_bulk(self.h, op, _p64(keys), _p64(vals), len(keys), _p64(out), _p8(ok), _p8(found))
+        return ok.astype(bool), out, found.astype(bool)
+
+    def count_fill(self, level: int) -> int:
+        return lib().pgo_btable_count_fill(self.h, level)

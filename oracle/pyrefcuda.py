@@ -11,8 +11,11 @@ import ctypes as C
 
 from . import pyoracle
 
-KIND_HT_DOUBLE_B8, KIND_HT_ALIAS, KIND_HT_LINEAR_B8, KIND_HT_P2_B8, KIND_TCF, KIND_TCQF = range(6)
+KIND_HT_DOUBLE_B8, KIND_HT_ALIAS, KIND_HT_LINEAR_B8, KIND_HT_P2_B8, KIND_TCF, KIND_TCQF, KIND_DEL_TCF, \
+    KIND_DEL_TCF_SMALL = range(8)
 OP_INSERT, OP_QUERY, OP_REMOVE = 0, 1, 2
+# bucketed filters (kinds 6, 7) take these too
+OP_INSERT_DELETE, OP_INSERT_IF_NOT_EXISTS, OP_INSERT_IF_NOT_EXISTS_DELETE = 3, 4, 5
 
 _lib = None
 
@@ -33,6 +36,8 @@ def lib():
         L.refc_destroy.argtypes = [V]
         L.refc_bulk.restype = C.c_int
         L.refc_bulk.argtypes = [V, C.c_int, V, V, C.c_uint64, V, V, C.c_int, V]
+        L.refc_bbulk.restype = C.c_int
+        L.refc_bbulk.argtypes = [V, C.c_int, V, V, C.c_uint64, V, V, V, C.c_int, V]
         L.refc_level.restype = C.c_int
         L.refc_level.argtypes = [V, C.c_int, C.POINTER(V), C.POINTER(C.c_uint64)]
         L.refc_dump.restype = C.c_int
@@ -68,6 +73,14 @@ class RefTable:
         r = lib().refc_bulk(self.h, op, _p(keys), _p(vals), keys.numel(), _p(flags), _p(vals_out), int(serial), st)
         if r != 0:
             raise RuntimeError("refc_bulk launch failed")
+
+    def bbulk(self, op, keys, vals=None, ok=None, vals_out=None, found=None, serial=False, stream=None):
+        """All six operations of the bucketed filters (kinds 6, 7)."""
+        st = None if stream is None else stream.cuda_stream
+        r = lib().refc_bbulk(self.h, op, _p(keys), _p(vals), keys.numel(), _p(ok), _p(vals_out), _p(found),
+                             int(serial), st)
+        if r != 0:
+            raise RuntimeError("refc_bbulk launch failed")
 
     def level(self, level: int):
         p = C.c_void_p()

@@ -25,6 +25,14 @@ CASES = {
 
 VAL_BYTES = {0: 8, 1: 2, 2: 0}
 
+# Bucketed filters with tombstone reuse (tests/src/delete_tests.cu:138-179):
+# tag bits, [(nslots, bucket, max_probes, scheme, probe), ...], seed.
+# schemes: 2 two-choice shortcut over packed buckets, 3 linear over packed buckets
+BCASES = {
+    "del_tcf": (16, [(4096, 16, 2, 2, 3), (4096 // 100 + 64, 8, 4000, 3, 1)], 42),
+    "del_tcf_small": (8, [(4096, 16, 2, 2, 3), (4096 // 100 + 64, 8, 400, 3, 1)], 42),
+}
+
 
 def golden(name: str):
     import numpy as np
@@ -43,3 +51,8 @@ def product_config(pg, name: str, tile: int | None = None):
     fmt, t, levels, seed = CASES[name]
     cfg = pg.TableConfig(fmt, tile or t, [pg.Level(*lv) for lv in levels])
     return cfg, seed
+
+
+def oracle_btable(oracle, name: str):
+    bits, levels, seed = BCASES[name]
+    return oracle.OracleBucketed(bits, levels, seed)

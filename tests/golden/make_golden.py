@@ -214,15 +214,140 @@ def ht_exceptions(okn, vals, half, rem_idx, found, vv, rok, found2, vv2):
             "found_after_remove": int(found2.astype(bool).sum())}
 
 
+# bucketed filters with tombstone reuse: name, kind, primary slots, backing slots, seed, #keys, key seed, tag bits
+BCASES = [
+    ("del_tcf", rc.KIND_DEL_TCF, 4096, 4096 // 100 + 64, 42, 3700, 1101, 16),
+    ("del_tcf_small", rc.KIND_DEL_TCF_SMALL, 4096, 4096 // 100 + 64, 42, 3700, 1102, 8),
+]
+BOPS = ("insert", "query", "remove", "insert_delete", "insert_if_not_exists", "insert_if_not_exists_delete")
+
+
+def blevels(n0: int, n1: int, tag_bits: int) -> list[int]:
+    w = 4 if tag_bits == 16 else 2
+    return [((n0 - 1) // 16 + 1) * 16 * w, ((n1 - 1) // 8 + 1) * 8 * w]
+
+
+def run_bcase(torch, name, kind, n0, n1, seed, nkeys, kseed, bits):
+    """A serial script of all six operations on a bucketed filter: insert to
+    0.9 load (overflowing into the backing table), query, remove a third,
+    re-add through insert_with_delete, insert_if_not_exists over a mix of
+    present and absent keys, insert_if_not_exists_delete likewise.  Every
+    step's results and the slot arrays after each step are recorded."""
+    dev = torch.device("cuda")
+    base = wl.keys_without_sentinels(kseed, nkeys)
+    mask = (1 << bits) - 1
+    edge = np.array([0, U64MAX, int(base[5]), 0x1234_0000_0000_0000, 0xABCD_0000_0000_0000 | mask,
+                     (int(base[7]) & ~mask) | 1], dtype=np.uint64)
+    keys = np.concatenate([base, edge])
+    vals = wl.values_for(keys, 2, seed=kseed + 7).astype(np.uint64) & np.uint64(mask)
+    fresh = wl.keys_without_sentinels(kseed + 500, 400)
+    vdt, vnp = (torch.int16, np.int16) if bits == 16 else (torch.uint8, np.uint8)
+    t = rc.RefTable(kind, n0, n1, seed)
+    sizes = blevels(n0, n1, bits)
+    rec = dict(kind=kind, n0=n0, n1=n1, seed=seed, bits=bits)
+
+    def run(step, op, k, v=None):
+        d_k = torch.from_numpy(np.ascontiguousarray(k).view(np.int64)).to(dev)
+        d_v = None if v is None else torch.from_numpy(np.ascontiguousarray(v).astype(np.uint64).astype(
+            np.uint16 if bits == 16 else np.uint8).view(vnp)).to(dev)
+        ok = torch.zeros(len(k), dtype=torch.uint8, device=dev)
+        out = torch.zeros(len(k), dtype=vdt, device=dev)
+        fd = torch.zeros(len(k), dtype=torch.uint8, device=dev)
+        t.bbulk(op, d_k, d_v, ok, out, fd, serial=True)
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()
+        o = (o.view(np.uint16) if bits == 16 else o).astype(np.uint64)
+        rec[f"s{step}_op"] = np.array([op])
+        rec[f"s{step}_keys"] = np.ascontiguousarray(k)
+        rec[f"s{step}_vals"] = np.zeros(len(k), dtype=np.uint64) if v is None else np.ascontiguousarray(v).astype(np.uint64)
+        rec[f"s{step}_ok"] = ok.cpu().numpy()
+        rec[f"s{step}_out"] = o
+        rec[f"s{step}_found"] = fd.cpu().numpy()
+        for l, b in enumerate(sizes):
+            rec[f"s{step}_dump_l{l}"] = np.frombuffer(t.dump(l, b), dtype=np.uint8)
+
+    third = nkeys // 3
+    mix = np.concatenate([keys[:200], fresh[:200]])
+    mix2 = np.concatenate([keys[200:400], fresh[200:400]])
+    mvals = (vals[:400] ^ np.uint64(0x5A)) & np.uint64(mask)
+    run(0, rc.OP_INSERT, keys, vals)
+    run(1, rc.OP_QUERY, np.concatenate([keys, fresh]))
+    run(2, rc.OP_REMOVE, np.concatenate([keys[:third], fresh[:20]]))
+    run(3, rc.OP_QUERY, np.concatenate([keys, fresh]))
+    run(4, rc.OP_INSERT_DELETE, keys[: third // 2], vals[: third // 2])
+    run(5, rc.OP_QUERY, np.concatenate([keys, fresh]))
+    run(6, rc.OP_INSERT_IF_NOT_EXISTS, mix, mvals)
+    run(7, rc.OP_INSERT_IF_NOT_EXISTS_DELETE, mix2, mvals)
+    run(8, rc.OP_QUERY, np.concatenate([keys, fresh]))
+    rec["steps"] = np.array([9])
+    t.close()
+    return rec
+
+
+def btcf_stats(torch, kind, bits):
+    """The reference's delete test flow (tests/src/delete_tests.cu:568-760) with
+    its parallel kernels at 2^22 primary slots + 1% backing, 0.9 load: insert
+    all, remove the first half, query the second half, re-add the first half
+    with insert_with_delete.  Records the counts that test prints."""
+    dev = torch.device("cuda")
+    n0 = 1 << 22
+    n1 = n0 // 100
+    n = int(0.9 * (n0 + n1))
+    mask = (1 << bits) - 1
+    keys = wl.keys_without_sentinels(42, n)
+    vals = wl.values_for(keys, 2, seed=49).astype(np.uint64) & np.uint64(mask)
+    vdt, vnp = (torch.int16, np.int16) if bits == 16 else (torch.uint8, np.uint8)
+    t = rc.RefTable(kind, n0, n1, 42)
+    d_k = torch.from_numpy(keys.view(np.int64)).to(dev)
+    d_v = torch.from_numpy(vals.astype(np.uint16 if bits == 16 else np.uint8).view(vnp)).to(dev)
+    half = n // 2
+    ok = torch.zeros(n, dtype=torch.uint8, device=dev)
+    t.bbulk(rc.OP_INSERT, d_k, d_v, ok)
+    rok = torch.zeros(half, dtype=torch.uint8, device=dev)
+    t.bbulk(rc.OP_REMOVE, d_k[:half].contiguous(), None, rok)
+    qf = torch.zeros(n - half, dtype=torch.uint8, device=dev)
+    qv = torch.zeros(n - half, dtype=vdt, device=dev)
+    t.bbulk(rc.OP_QUERY, d_k[half:].contiguous(), None, qf, qv)
+    aok = torch.zeros(half, dtype=torch.uint8, device=dev)
+    t.bbulk(rc.OP_INSERT_DELETE, d_k[:half].contiguous(), d_v[:half].contiguous(), aok)
+    af = torch.zeros(n, dtype=torch.uint8, device=dev)
+    t.bbulk(rc.OP_QUERY, d_k, None, af)
+    torch.cuda.synchronize()
+    okn = ok.cpu().numpy().astype(bool)
+    qvn = qv.cpu().numpy()
+    qvn = (qvn.view(np.uint16) if bits == 16 else qvn).astype(np.uint64)
+    qfn = qf.cpu().numpy().astype(bool)
+    t.close()
+    return {"workload": f"bucketed filter ({bits}-bit tags) 2^22 slots + 1% backing, 0.9 load, seeds 42/49",
+            "inserted": n, "insert_failures": int((~okn).sum()),
+            "remove_misses": int((~rok.cpu().numpy().astype(bool)).sum()),
+            "query_misses": int((~qfn & okn[half:]).sum()),
+            "query_value_mismatches": int((qfn & (qvn != vals[half:])).sum()),
+            "readd_failures": int((~aok.cpu().numpy().astype(bool)).sum()),
+            "found_after_readd": int(af.cpu().numpy().astype(bool).sum())}
+
+
 def main():
     import torch
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(ROOT / "tests" / "golden"))
     ap.add_argument("--skip-stats", action="store_true")
+    ap.add_argument("--bucketed-only", action="store_true", help="only the bucketed filter cases and stats")
     a = ap.parse_args()
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
+    for case in BCASES:
+        rec = run_bcase(torch, *case)
+        np.savez_compressed(out / f"ref_{case[0]}.npz", **rec)
+        print(case[0], "inserted", int(rec["s0_ok"].sum()), "/", len(rec["s0_keys"]))
+    if a.bucketed_only:
+        if not a.skip_stats:
+            bstats = {"del_tcf": btcf_stats(torch, rc.KIND_DEL_TCF, 16),
+                      "del_tcf_small": btcf_stats(torch, rc.KIND_DEL_TCF_SMALL, 8)}
+            (out / "ref_bucketed_stats.json").write_text(json.dumps(bstats, indent=1))
+            print(json.dumps(bstats, indent=1))
+        return
     for case in CASES:
         rec = run_case(torch, *case)
         np.savez_compressed(out / f"ref_{case[0]}.npz", **rec)
@@ -231,6 +356,10 @@ def main():
         stats = {"tcf": tcf_stats(torch), "ht": ht_stats(torch)}
         (out / "ref_stats.json").write_text(json.dumps(stats, indent=1))
         print(json.dumps(stats, indent=1))
+        bstats = {"del_tcf": btcf_stats(torch, rc.KIND_DEL_TCF, 16),
+                  "del_tcf_small": btcf_stats(torch, rc.KIND_DEL_TCF_SMALL, 8)}
+        (out / "ref_bucketed_stats.json").write_text(json.dumps(bstats, indent=1))
+        print(json.dumps(bstats, indent=1))
 
 
 if __name__ == "__main__":

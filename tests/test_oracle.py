@@ -10,7 +10,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from tests.cases import CASES, golden, oracle_table
+from tests.cases import BCASES, CASES, golden, oracle_btable, oracle_table
 from poggers_b200 import workload as wl
 
 
@@ -165,3 +165,41 @@ def test_multithreaded_port_tcf_no_false_negatives(oracle):
     ok = t.insert_many(keys, wl.values_for(keys, 2, 1).astype(np.uint64), threads=4)
     f, _ = t.query_many(keys, threads=4)
     assert (f | ~ok).all()
+
+
+@pytest.mark.parametrize("name", sorted(BCASES))
+def test_bucketed_oracle_matches_reference_golden(oracle, name):
+    """Every step of the recorded script (insert, query, remove, insert_with_delete,
+    insert_if_not_exists, insert_if_not_exists_delete): results and both levels'
+    bytes equal the reference's."""
+    g = golden(name)
+    if g is None:
+        pytest.skip(f"golden fixture ref_{name}.npz not recorded yet")
+    o = oracle_btable(oracle, name)
+    for s in range(int(g["steps"][0])):
+        ok, out, fd = o.bulk(int(g[f"s{s}_op"][0]), g[f"s{s}_keys"], g[f"s{s}_vals"])
+        assert (ok == g[f"s{s}_ok"].astype(bool)).all(), f"step {s} ok"
+        assert (out == g[f"s{s}_out"]).all(), f"step {s} values"
+        assert (fd == g[f"s{s}_found"].astype(bool)).all(), f"step {s} found"
+        for l in range(2):
+            assert o.level_bytes(l) == g[f"s{s}_dump_l{l}"].tobytes(), f"step {s} level {l} bytes"
+
+
+def test_bucketed_tags_and_tombstone_reuse(oracle):
+    """Tags move 0 and all-ones off the sentinels; a removed slot is reused only
+    by insert_with_delete; insert_if_not_exists reports the stored value."""
+    assert oracle.lib().pgo_btag(16, 0x10000) == 1 and oracle.lib().pgo_btag(16, 0xFFFF) == 0xFFFE
+    assert oracle.lib().pgo_btag(8, 0x100) == 1 and oracle.lib().pgo_btag(8, 0x1FF) == 0xFE
+    o = oracle.OracleBucketed(16, [(16, 16, 2, 2, 3)], 7)
+    keys = wl.keys_without_sentinels(5, 16)
+    ok, _, _ = o.bulk(oracle.BOP_INSERT, keys, keys & np.uint64(0xFF))
+    assert ok.sum() >= 12 and o.count_fill(0) == ok.sum()
+    placed = keys[ok]
+    r, _, _ = o.bulk(oracle.BOP_REMOVE, placed[:4])
+    assert r.all() and o.count_fill(0) == ok.sum() - 4
+    new = wl.keys_without_sentinels(6, 4)
+    before = o.level_bytes(0)
+    ok2, _, _ = o.bulk(oracle.BOP_INSERT_DELETE, new, np.arange(4, dtype=np.uint64))
+    assert ok2.all() and o.level_bytes(0) != before
+    f, v, found = o.bulk(oracle.BOP_INSERT_IF_NOT_EXISTS, new[:1], np.array([99], dtype=np.uint64))
+    assert f[0] and found[0] and v[0] == 0
