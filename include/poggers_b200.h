@@ -18,7 +18,8 @@
  *  - Counters passed as d_count are ADDED to (like the reference test
  *    harness's atomicAdd on a caller-zeroed counter); zero them first.
  *  - Values are typed by the table format: uint64_t for PG_FMT_KV64,
- *    uint16_t for PG_FMT_TAGVAL16; PG_FMT_TAG16 stores no values and reports
+ *    uint16_t for PG_FMT_TAGVAL16 and PG_FMT_PACKED_TAGVAL16, uint8_t for
+ *    PG_FMT_PACKED_TAGVAL8; PG_FMT_TAG16 stores no values and reports
  *    0, like key_container::get_val (representations/key_only.cuh:75-77).
  *
  * Reference interfaces replaced (paths inside the reference project):
@@ -33,6 +34,10 @@
  *                        (driver: tests/src/delete_tests.cu:336-372)
  *   pg_table_count_fill <- count_fill_kernel / get_fill                       tables/bucketed_table.cuh:37-52,498-548
  *   pg_table_bytes    <- host_bytes_in_use                                    tables/base_table.cuh:331-351
+ *   pg_bulk_insert_with_delete <- bucketed_table::insert_with_delete          tables/bucketed_table.cuh:222-240
+ *                        (driver: tests/src/delete_tests.cu:274-296)
+ *   pg_bulk_insert_if_not_exists[_delete] <- bucketed_table::insert_if_not_exists[_delete]
+ *                                                                             tables/bucketed_table.cuh:188-220
  */
 #ifndef POGGERS_B200_H
 #define POGGERS_B200_H
@@ -62,13 +67,22 @@ typedef enum pg_status {
 enum {
     PG_FMT_KV64 = 0,     /* key_val_pair<uint64_t,uint64_t>: the modular hash tables */
     PG_FMT_TAGVAL16 = 1, /* dynamic_container<key_val_pair,uint16_t>: the TCF (16-bit tag + 16-bit val) */
-    PG_FMT_TAG16 = 2     /* dynamic_container<key_container,uint16_t>: tag-only TCF */
+    PG_FMT_TAG16 = 2,    /* dynamic_container<key_container,uint16_t>: tag-only TCF */
+    /* the bucketed filter with tombstone reuse: bucketed_internal_dynamic_container
+     * of grouped_bits_pair slots, one CAS-able word per slot (tag low, value high);
+     * used with the *_BUCKETED schemes on every level (tests/src/delete_tests.cu:138-179) */
+    PG_FMT_PACKED_TAGVAL16 = 3, /* grouped_bits_pair<16,16>: 4-byte slots (del_TCF) */
+    PG_FMT_PACKED_TAGVAL8 = 4   /* grouped_bits_pair<8,8>: 2-byte slots (del_TCF_small) */
 };
 
 /* insert schemes */
 enum {
     PG_SCHEME_BUCKET = 0,     /* insert_schemes/bucket_insert.cuh */
-    PG_SCHEME_TWO_CHOICE = 1  /* insert_schemes/power_of_n_shortcut.cuh (max_probes <= 8) */
+    PG_SCHEME_TWO_CHOICE = 1, /* insert_schemes/power_of_n_shortcut.cuh (max_probes <= 4) */
+    PG_SCHEME_TWO_CHOICE_BUCKETED = 2, /* insert_schemes/power_of_n_shortcut_buckets.cuh (max_probes <= 4,
+                                          bucket 8/16/32; packed formats only) */
+    PG_SCHEME_LINEAR_BUCKETED = 3      /* insert_schemes/linear_insert_buckets.cuh (packed formats only;
+                                          bucket 8/16/32 as primary, 8/16 as backing) */
 };
 
 /* probing schemes */
@@ -172,7 +186,27 @@ pg_status pg_bulk_query(pg_table *t, const uint64_t *d_keys, uint64_t n, void *d
 pg_status pg_bulk_remove(pg_table *t, const uint64_t *d_keys, uint64_t n, uint8_t *d_ok,
                          uint64_t *d_hit_count, pg_stream_t stream);
 
-/* d_out[0] += occupied (non-empty) slots of `level`, d_out[1] += tombstones. */
+/* Bucketed filter (packed formats) only; other formats return PG_ERR_UNSUPPORTED,
+ * as the reference's static_table schemes have no such methods.
+ *
+ * insert_with_delete: like pg_bulk_insert, but a deleted slot may be reused
+ * (packed_bucket.cuh:116-180).  d_ok / d_fail_count as for pg_bulk_insert. */
+pg_status pg_bulk_insert_with_delete(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                     uint8_t *d_ok, uint64_t *d_fail_count, pg_stream_t stream);
+/* insert_if_not_exists: a key already present is reported (d_found[i] = 1,
+ * d_vals_out[i] = its value) and not inserted again; otherwise it is inserted.
+ * d_ok[i] = 1 when found or inserted; d_fail_count += keys neither found nor
+ * inserted.  The _delete form removes a key it finds instead (the
+ * reference's find-and-delete), reusing deleted slots when it inserts. */
+pg_status pg_bulk_insert_if_not_exists(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                       void *d_vals_out, uint8_t *d_found, uint8_t *d_ok, uint64_t *d_fail_count,
+                                       pg_stream_t stream);
+pg_status pg_bulk_insert_if_not_exists_delete(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                              void *d_vals_out, uint8_t *d_found, uint8_t *d_ok,
+                                              uint64_t *d_fail_count, pg_stream_t stream);
+
+/* d_out[0] += occupied (non-empty) slots of `level`, d_out[1] += tombstones.
+ * The bucketed filter's get_fill (live slots) is d_out[0] - d_out[1]. */
 pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_stream_t stream);
 
 /* Copy a level to / from host memory in the REFERENCE's slot layout

@@ -53,7 +53,9 @@ enum fmt_kind : uint32_t {
     FMT_TAG16 = 2,
     FMT_KV64_SPLIT = 3,
     FMT_TAGVAL16_SPLIT = 4,
-    FMT_KV64_FP = 5
+    FMT_KV64_FP = 5,
+    FMT_PACKED16 = 6,  // bucketed filter, 16-bit tag + 16-bit value words (packed.cuh)
+    FMT_PACKED8 = 7    // bucketed filter, 8-bit tag + 8-bit value words
 };
 enum scheme_kind : uint32_t { SCHEME_BUCKET = 0, SCHEME_TWO_CHOICE = 1 };
 

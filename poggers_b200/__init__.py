@@ -35,11 +35,12 @@ PG_STATIC_MAX_TABLES = 256
 PG_STATIC_MAX_OPS = 8192
 PG_TABLE_SPLIT_BUCKETS = 1
 PG_TABLE_FINGERPRINTS = 2
-FMT_KV64, FMT_TAGVAL16, FMT_TAG16 = 0, 1, 2
-SCHEME_BUCKET, SCHEME_TWO_CHOICE = 0, 1
+FMT_KV64, FMT_TAGVAL16, FMT_TAG16, FMT_PACKED_TAGVAL16, FMT_PACKED_TAGVAL8 = 0, 1, 2, 3, 4
+SCHEME_BUCKET, SCHEME_TWO_CHOICE, SCHEME_TWO_CHOICE_BUCKETED, SCHEME_LINEAR_BUCKETED = 0, 1, 2, 3
 PROBE_DOUBLE, PROBE_LINEAR, PROBE_P2, PROBE_XOR_P2 = 0, 1, 2, 3
-KEY_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 2}
-VAL_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 0}
+KEY_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 2, FMT_PACKED_TAGVAL16: 2, FMT_PACKED_TAGVAL8: 1}
+VAL_BYTES = {FMT_KV64: 8, FMT_TAGVAL16: 2, FMT_TAG16: 0, FMT_PACKED_TAGVAL16: 2, FMT_PACKED_TAGVAL8: 1}
+PACKED_FORMATS = (FMT_PACKED_TAGVAL16, FMT_PACKED_TAGVAL8)
 SLOT_BYTES = {f: KEY_BYTES[f] + VAL_BYTES[f] for f in KEY_BYTES}
 
 
@@ -79,7 +80,8 @@ _lib = None
 EXPORTED = (
     "pg_version", "pg_status_string", "pg_table_create", "pg_table_destroy", "pg_table_clear",
     "pg_table_level_info", "pg_table_bytes", "pg_table_set_launch", "pg_table_set_partitioned_insert",
-    "pg_bulk_insert", "pg_bulk_query",
+    "pg_bulk_insert", "pg_bulk_insert_with_delete", "pg_bulk_insert_if_not_exists",
+    "pg_bulk_insert_if_not_exists_delete", "pg_bulk_query",
     "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
@@ -122,6 +124,11 @@ def lib() -> C.CDLL:
     L.pg_bulk_insert.argtypes = [V, P, P, U64, P, P, P]
     L.pg_bulk_query.restype = C.c_int
     L.pg_bulk_query.argtypes = [V, P, U64, P, P, P, P]
+    L.pg_bulk_insert_with_delete.restype = C.c_int
+    L.pg_bulk_insert_with_delete.argtypes = [V, P, P, U64, P, P, P]
+    for f in ("pg_bulk_insert_if_not_exists", "pg_bulk_insert_if_not_exists_delete"):
+        getattr(L, f).restype = C.c_int
+        getattr(L, f).argtypes = [V, P, P, U64, P, P, P, P, P]
     L.pg_bulk_remove.restype = C.c_int
     L.pg_bulk_remove.argtypes = [V, P, U64, P, P, P]
     L.pg_table_count_fill.restype = C.c_int
@@ -321,6 +328,8 @@ class Table:
     def serial(self, lanes_per_key: int = 0) -> None:
         """One group walks the batch in order (deterministic layout, for parity checks)."""
         lanes = 1 if self.config.fingerprints else (lanes_per_key or self.config.tile)
+        if self.format in PACKED_FORMATS:
+            lanes = 4 if lanes >= 4 else 1  # the widths the bucketed filter's kernels are built for
         self.set_launch(lanes, 1, 1, lanes)
 
     def level_info(self, level: int) -> dict:
@@ -346,6 +355,21 @@ class Table:
         n = keys.numel() if n is None else n
         _check(lib().pg_bulk_remove(self._h, _ptr(keys), n, _ptr(ok), _ptr(hit_count), _stream(stream)),
                "pg_bulk_remove")
+
+    def bulk_insert_with_delete(self, keys, vals=None, ok=None, fail_count=None, stream=None,
+                                n: int | None = None) -> None:
+        """bucketed_table::insert_with_delete: deleted slots may be reused (packed formats)."""
+        n = keys.numel() if n is None else n
+        _check(lib().pg_bulk_insert_with_delete(self._h, _ptr(keys), _ptr(vals), n, _ptr(ok), _ptr(fail_count),
+                                                _stream(stream)), "pg_bulk_insert_with_delete")
+
+    def bulk_insert_if_not_exists(self, keys, vals=None, vals_out=None, found=None, ok=None, fail_count=None,
+                                  stream=None, n: int | None = None, delete: bool = False) -> None:
+        """bucketed_table::insert_if_not_exists (delete=True: insert_if_not_exists_delete)."""
+        n = keys.numel() if n is None else n
+        fn = lib().pg_bulk_insert_if_not_exists_delete if delete else lib().pg_bulk_insert_if_not_exists
+        _check(fn(self._h, _ptr(keys), _ptr(vals), n, _ptr(vals_out), _ptr(found), _ptr(ok), _ptr(fail_count),
+                  _stream(stream)), "pg_bulk_insert_if_not_exists")
 
     def count_fill(self, level: int, out, stream=None) -> None:
         """out (2 x uint64 device) += [occupied slots, tombstones] of `level`."""
@@ -397,6 +421,19 @@ class data_structs:
                       max_probes: int = 20) -> TableConfig:
         # data_structs/uint64_hash_table.cuh:35
         return TableConfig(FMT_KV64, tile, [Level(nslots, bucket, max_probes, SCHEME_BUCKET, probe)])
+
+    @staticmethod
+    def del_tcf(nslots: int, backing_nslots: int, tile: int = 4, tag_bits: int = 16) -> TableConfig:
+        """The bucketed filter with tombstone reuse of tests/src/delete_tests.cu:138-179:
+        packed (tag, value) slots, two-choice shortcut over 16-slot buckets with
+        XOR power-of-two probing, backed by an 8-slot linear-probing table
+        (4000 probes; 400 for 8-bit tags, del_TCF_small)."""
+        fmt = FMT_PACKED_TAGVAL16 if tag_bits == 16 else FMT_PACKED_TAGVAL8
+        levels = [Level(nslots, 16, 2, SCHEME_TWO_CHOICE_BUCKETED, PROBE_XOR_P2)]
+        if backing_nslots:
+            levels.append(Level(backing_nslots, 8, 4000 if tag_bits == 16 else 400, SCHEME_LINEAR_BUCKETED,
+                                PROBE_LINEAR))
+        return TableConfig(fmt, tile, levels)
 
     @staticmethod
     def two_choice_table_64(nslots: int, tile: int = 4, bucket: int = 8) -> TableConfig:

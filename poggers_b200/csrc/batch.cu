@@ -121,6 +121,7 @@ pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t ma
     *out = nullptr;
     const pg_table *t0 = tables[0];
     if (!t0) return PG_ERR_INVALID;
+    if (t0->ifmt == FMT_PACKED16 || t0->ifmt == FMT_PACKED8) return PG_ERR_UNSUPPORTED;  // bulk calls only
     for (uint32_t i = 1; i < ntables; i++) {
         const pg_table *t = tables[i];
         // one kernel instantiation serves the batch: same format, bucket, scheme and depth
@@ -228,6 +229,7 @@ pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const p
     if (ntables > kStaticMaxTables || max_ops > kStaticMaxOps) return PG_ERR_TOO_LARGE;
     const pg_table *t0 = tables[0];
     if (!t0) return PG_ERR_INVALID;
+    if (t0->ifmt == FMT_PACKED16 || t0->ifmt == FMT_PACKED8) return PG_ERR_UNSUPPORTED;  // bulk calls only
     for (uint32_t i = 1; i < ntables; i++) {
         const pg_table *t = tables[i];
         if (!t || t->ifmt != t0->ifmt || t->cfg.levels[0].bucket_size != t0->cfg.levels[0].bucket_size ||

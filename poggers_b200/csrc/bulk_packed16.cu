@@ -1,0 +1,12 @@
+// bulk_packed16.cu -- bulk kernels of the bucketed filter with 16-bit tags and values.
+#include "bulk_packed.cuh"
+
+namespace pg {
+
+cudaError_t launch_packed16(int op, uint32_t b0, uint32_t b1, uint32_t lanes, const table_desc &t,
+                            const packed_args &a, dim3 grid, dim3 block, cudaStream_t s)
+{
+    return launch_packed<16>(op, b0, b1, lanes, t, a, grid, block, s);
+}
+
+}  // namespace pg

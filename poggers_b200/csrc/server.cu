@@ -400,6 +400,7 @@ pg_status pg_server_destroy(pg_server *s)
 pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t seed, uint32_t *table_id)
 {
     if (!s || !cfg || !table_id) return PG_ERR_INVALID;
+    if (cfg->format == PG_FMT_PACKED_TAGVAL16 || cfg->format == PG_FMT_PACKED_TAGVAL8) return PG_ERR_UNSUPPORTED;
     // admission by HBM budget: the table's slot arrays (and fingerprints) must fit
     uint64_t need = 0;
     const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : 2, vb = cfg->format == PG_FMT_KV64 ? 8 : (cfg->format == PG_FMT_TAGVAL16 ? 2 : 0);

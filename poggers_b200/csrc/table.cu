@@ -7,6 +7,7 @@
 
 #include "poggers_b200.h"
 #include "bulk_kernels.cuh"
+#include "bulk_packed.cuh"
 
 using namespace pg;
 
@@ -14,8 +15,21 @@ using namespace pg;
 
 namespace {
 
-uint32_t key_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : 2u; }
-uint32_t val_bytes(uint32_t fmt) { return fmt == PG_FMT_KV64 ? 8u : (fmt == PG_FMT_TAGVAL16 ? 2u : 0u); }
+bool packed(uint32_t fmt) { return fmt == PG_FMT_PACKED_TAGVAL16 || fmt == PG_FMT_PACKED_TAGVAL8; }
+uint32_t key_bytes(uint32_t fmt)
+{
+    return fmt == PG_FMT_KV64 ? 8u : (fmt == PG_FMT_PACKED_TAGVAL8 ? 1u : 2u);
+}
+uint32_t val_bytes(uint32_t fmt)
+{
+    switch (fmt) {
+    case PG_FMT_KV64: return 8u;
+    case PG_FMT_TAGVAL16:
+    case PG_FMT_PACKED_TAGVAL16: return 2u;
+    case PG_FMT_PACKED_TAGVAL8: return 1u;
+    default: return 0u;
+    }
+}
 
 bool split_layout(const pg_table_config *c)
 {
@@ -29,6 +43,8 @@ bool fingerprinted(const pg_table_config *c)
 
 uint32_t internal_format(const pg_table_config *c)
 {
+    if (c->format == PG_FMT_PACKED_TAGVAL16) return FMT_PACKED16;
+    if (c->format == PG_FMT_PACKED_TAGVAL8) return FMT_PACKED8;
     if (fingerprinted(c)) return FMT_KV64_FP;
     if (!split_layout(c)) return c->format;
     return c->format == PG_FMT_KV64 ? (uint32_t)FMT_KV64_SPLIT : (uint32_t)FMT_TAGVAL16_SPLIT;
@@ -43,9 +59,30 @@ pg_status validate(const pg_table_config *c)
             c->levels[0].scheme != PG_SCHEME_BUCKET)
             return PG_ERR_UNSUPPORTED;
     }
-    if (c->format > PG_FMT_TAG16) return PG_ERR_INVALID;
+    if (c->format > PG_FMT_PACKED_TAGVAL8) return PG_ERR_INVALID;
     if (c->nlevels < 1 || c->nlevels > 2) return PG_ERR_INVALID;
     if (!(c->tile == 1 || c->tile == 2 || c->tile == 4 || c->tile == 8 || c->tile == 16)) return PG_ERR_INVALID;
+    if (packed(c->format)) {
+        // the bucketed filter: packed slots with the bucketed schemes on every level
+        if (c->flags) return PG_ERR_UNSUPPORTED;
+        for (uint32_t l = 0; l < c->nlevels; l++) {
+            const pg_level_config &L = c->levels[l];
+            if (L.nslots == 0 || L.bucket_size == 0 || L.max_probes == 0 || L.probe > PG_PROBE_XOR_P2)
+                return PG_ERR_INVALID;
+            if (L.scheme != PG_SCHEME_TWO_CHOICE_BUCKETED && L.scheme != PG_SCHEME_LINEAR_BUCKETED)
+                return PG_ERR_INVALID;
+            if ((L.probe == PG_PROBE_P2 || L.probe == PG_PROBE_XOR_P2) && L.max_probes != 2) return PG_ERR_INVALID;
+            if (L.scheme == PG_SCHEME_TWO_CHOICE_BUCKETED && L.max_probes > (uint32_t)kTwoChoiceMaxProbes)
+                return PG_ERR_UNSUPPORTED;
+            if (L.nslots / L.bucket_size > (1ULL << 40)) return PG_ERR_INVALID;
+        }
+        const uint32_t b0 = c->levels[0].bucket_size;
+        if (!(b0 == 8 || b0 == 16 || b0 == 32)) return PG_ERR_UNSUPPORTED;
+        if (c->nlevels > 1 && !(c->levels[1].bucket_size == 8 || c->levels[1].bucket_size == 16))
+            return PG_ERR_UNSUPPORTED;
+        if (c->tile > b0) return PG_ERR_UNSUPPORTED;
+        return PG_OK;
+    }
     for (uint32_t l = 0; l < c->nlevels; l++) {
         const pg_level_config &L = c->levels[l];
         if (L.nslots == 0 || L.bucket_size == 0 || L.max_probes == 0) return PG_ERR_INVALID;
@@ -108,6 +145,26 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     return cuda_status(e);
 }
 
+// the bucketed filter's operations (packed formats)
+pg_status run_packed(pg_table *t, int op, const packed_args &a, pg_stream_t stream)
+{
+    if (!t) return PG_ERR_INVALID;
+    if (t->ifmt != FMT_PACKED16 && t->ifmt != FMT_PACKED8) return PG_ERR_UNSUPPORTED;
+    if (a.n == 0) return PG_OK;
+    if (!a.keys) return PG_ERR_INVALID;
+    // one group per key, blocks in batch order like the reference's one-tile-per-key
+    // launch: with deletes in the mix, which of two keys sharing a tag holds the
+    // earlier slot (and so which one a remove takes) follows the batch order
+    dim3 grid, block;
+    launch_shape(t, a.n, grid, block, true);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t b0 = t->cfg.levels[0].bucket_size, b1 = t->cfg.nlevels > 1 ? t->cfg.levels[1].bucket_size : 8;
+    const uint32_t lanes = lanes_of(t);
+    const cudaError_t e = t->ifmt == FMT_PACKED16 ? launch_packed16(op, b0, b1, lanes, t->desc, a, grid, block, s)
+                                                  : launch_packed8(op, b0, b1, lanes, t->desc, a, grid, block, s);
+    return cuda_status(e);
+}
+
 // occupied / tombstone counts of one level: one thread per bucket
 template <class K>
 __global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, uint64_t nb, uint32_t B,
@@ -154,7 +211,9 @@ __global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, u
 // lanes a kernel uses per key for this table
 uint32_t pg_table_lanes(const pg_table *t)
 {
-    return t->ifmt == FMT_KV64_FP ? 1u : t->lanes;  // the fingerprint walk serves a key with one lane
+    if (t->ifmt == FMT_KV64_FP) return 1u;  // the fingerprint walk serves a key with one lane
+    if (t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8) return t->lanes >= 4 ? 4u : 1u;  // compiled widths
+    return t->lanes;
 }
 
 extern "C" {
@@ -314,6 +373,10 @@ pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t bloc
 pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n, uint8_t *d_ok,
                          uint64_t *d_fail_count, pg_stream_t stream)
 {
+    if (t && packed(t->cfg.format)) {
+        packed_args p{d_keys, d_vals, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_fail_count), n};
+        return run_packed(t, POP_INSERT, p, stream);
+    }
     bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
                 reinterpret_cast<unsigned long long *>(d_fail_count), n};
     if (t && d_keys && n) pg_partition_insert(t, a, reinterpret_cast<cudaStream_t>(stream));
@@ -323,6 +386,11 @@ pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals
 pg_status pg_bulk_query(pg_table *t, const uint64_t *d_keys, uint64_t n, void *d_vals_out, uint8_t *d_found,
                         uint64_t *d_hit_count, pg_stream_t stream)
 {
+    if (t && packed(t->cfg.format)) {
+        packed_args p{d_keys, nullptr, d_vals_out, d_found, nullptr, reinterpret_cast<unsigned long long *>(d_hit_count),
+                      n};
+        return run_packed(t, POP_QUERY, p, stream);
+    }
     bulk_args a{d_keys, nullptr, d_vals_out, d_found, reinterpret_cast<unsigned long long *>(d_hit_count), n};
     return run_bulk(t, OP_QUERY, a, stream);
 }
@@ -330,8 +398,35 @@ pg_status pg_bulk_query(pg_table *t, const uint64_t *d_keys, uint64_t n, void *d
 pg_status pg_bulk_remove(pg_table *t, const uint64_t *d_keys, uint64_t n, uint8_t *d_ok, uint64_t *d_hit_count,
                          pg_stream_t stream)
 {
+    if (t && packed(t->cfg.format)) {
+        packed_args p{d_keys, nullptr, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_hit_count), n};
+        return run_packed(t, POP_REMOVE, p, stream);
+    }
     bulk_args a{d_keys, nullptr, nullptr, d_ok, reinterpret_cast<unsigned long long *>(d_hit_count), n};
     return run_bulk(t, OP_REMOVE, a, stream);
+}
+
+pg_status pg_bulk_insert_with_delete(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                     uint8_t *d_ok, uint64_t *d_fail_count, pg_stream_t stream)
+{
+    packed_args p{d_keys, d_vals, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_fail_count), n};
+    return run_packed(t, POP_INSERT_DELETE, p, stream);
+}
+
+pg_status pg_bulk_insert_if_not_exists(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                       void *d_vals_out, uint8_t *d_found, uint8_t *d_ok, uint64_t *d_fail_count,
+                                       pg_stream_t stream)
+{
+    packed_args p{d_keys, d_vals, d_vals_out, d_ok, d_found, reinterpret_cast<unsigned long long *>(d_fail_count), n};
+    return run_packed(t, POP_INSERT_IF_NOT_EXISTS, p, stream);
+}
+
+pg_status pg_bulk_insert_if_not_exists_delete(pg_table *t, const uint64_t *d_keys, const void *d_vals, uint64_t n,
+                                              void *d_vals_out, uint8_t *d_found, uint8_t *d_ok,
+                                              uint64_t *d_fail_count, pg_stream_t stream)
+{
+    packed_args p{d_keys, d_vals, d_vals_out, d_ok, d_found, reinterpret_cast<unsigned long long *>(d_fail_count), n};
+    return run_packed(t, POP_INSERT_IF_NOT_EXISTS_DELETE, p, stream);
 }
 
 pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_stream_t stream)
@@ -350,6 +445,12 @@ pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_s
     if (t->cfg.format == PG_FMT_KV64)
         k_count_fill<unsigned long long><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
                                                                           stride, ~0ULL, out);
+    else if (t->cfg.format == PG_FMT_PACKED_TAGVAL16)  // whole words; the tombstone word is tag 0xFFFF, value 0
+        k_count_fill<unsigned int><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes, 4u,
+                                                                    0xFFFFu, out);
+    else if (t->cfg.format == PG_FMT_PACKED_TAGVAL8)
+        k_count_fill<unsigned short><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes, 2u,
+                                                                      (unsigned short)0x00FFu, out);
     else
         k_count_fill<unsigned short><<<(unsigned)blocks, 256, 0, s>>>(D.base, nb, D.bucket_size, D.bucket_bytes,
                                                                       stride, (unsigned short)0xFFFFu, out);

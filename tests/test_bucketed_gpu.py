@@ -1,0 +1,193 @@
+"""GPU parity tests of the bucketed filter with tombstone reuse (packed slots).
+
+Bar: in the serial launch shape every step of the script recorded from the
+reference's CUDA build (insert, query, remove, insert_with_delete,
+insert_if_not_exists, insert_if_not_exists_delete) gives the reference's
+results and the reference's bytes in both levels.  In the parallel shape the
+reference's delete-test flow gives no false negatives, no failed removes or
+re-adds, and tag-collision counts within a stated tolerance of the
+reference's own parallel run.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from tests.cases import BCASES, GOLDEN, golden
+from tests.gpu_util import to_dev
+from poggers_b200 import workload as wl
+
+pytestmark = pytest.mark.gpu
+
+OPS = ("insert", "query", "remove", "insert_delete", "insert_if_not_exists", "insert_if_not_exists_delete")
+
+
+def _table(pg, name):
+    bits, levels, seed = BCASES[name]
+    fmt = pg.FMT_PACKED_TAGVAL16 if bits == 16 else pg.FMT_PACKED_TAGVAL8
+    cfg = pg.TableConfig(fmt, 4, [pg.Level(*lv) for lv in levels])
+    return pg.Table(cfg, seed), bits
+
+
+def _vals_dev(bits, v):
+    import torch
+    if bits == 16:
+        return torch.from_numpy(np.ascontiguousarray(v).astype(np.uint16).view(np.int16)).cuda()
+    return torch.from_numpy(np.ascontiguousarray(v).astype(np.uint8)).cuda()
+
+
+def _run(pg, t, bits, op, keys, vals=None):
+    """One bulk operation; returns (ok, out values, found) as numpy."""
+    import torch
+    n = len(keys)
+    k = to_dev(np.ascontiguousarray(keys, dtype=np.uint64))
+    v = None if vals is None else _vals_dev(bits, vals)
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(n, dtype=torch.int16 if bits == 16 else torch.uint8, device="cuda")
+    fd = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    if op == 0:
+        t.bulk_insert(k, v, ok, cnt)
+    elif op == 1:
+        t.bulk_query(k, out, ok, cnt)
+    elif op == 2:
+        t.bulk_remove(k, ok, cnt)
+    elif op == 3:
+        t.bulk_insert_with_delete(k, v, ok, cnt)
+    else:
+        t.bulk_insert_if_not_exists(k, v, out, fd, ok, cnt, delete=(op == 5))
+    torch.cuda.synchronize()
+    okn = ok.cpu().numpy().astype(bool)
+    c = int(cnt.item())
+    assert c == (int(okn.sum()) if op in (1, 2) else int((~okn).sum())), "counter disagrees with the flags"
+    o = out.cpu().numpy()
+    o = (o.view(np.uint16) if bits == 16 else o).astype(np.uint64)
+    return okn, o, fd.cpu().numpy().astype(bool)
+
+
+@pytest.mark.parametrize("lanes", [1, 4])
+@pytest.mark.parametrize("name", sorted(BCASES))
+def test_serial_matches_reference_script_bytes(pg, name, lanes):
+    g = golden(name)
+    if g is None:
+        pytest.skip(f"golden fixture ref_{name}.npz not recorded yet")
+    t, bits = _table(pg, name)
+    t.serial(lanes)
+    for s in range(int(g["steps"][0])):
+        op = int(g[f"s{s}_op"][0])
+        vals = g[f"s{s}_vals"] if op in (0, 3, 4, 5) else None
+        ok, out, fd = _run(pg, t, bits, op, g[f"s{s}_keys"], vals)
+        assert (ok == g[f"s{s}_ok"].astype(bool)).all(), f"step {s} ({OPS[op]}) ok"
+        if op in (1, 4, 5):
+            assert (out == g[f"s{s}_out"]).all(), f"step {s} ({OPS[op]}) values"
+        if op in (4, 5):
+            assert (fd == g[f"s{s}_found"].astype(bool)).all(), f"step {s} ({OPS[op]}) found"
+        for lv in range(2):
+            assert t.dump_level(lv) == g[f"s{s}_dump_l{lv}"].tobytes(), f"step {s} ({OPS[op]}) level {lv} bytes"
+
+
+@pytest.mark.parametrize("name", sorted(BCASES))
+def test_parallel_matches_oracle_on_a_script(pg, oracle, name):
+    """Phase-separated parallel launches against the sequential oracle: every key
+    placed by both runs answers queries alike; removes and re-adds succeed for the
+    same keys; fill counts agree up to the keys whose placement differs."""
+    bits, levels, seed = BCASES[name]
+    t, _ = _table(pg, name)
+    o = oracle.OracleBucketed(bits, levels, seed)
+    n = 3000
+    keys = wl.keys_without_sentinels(77, n)
+    vals = wl.values_for(keys, 2, 3).astype(np.uint64) & np.uint64((1 << bits) - 1)
+    ok, _, _ = _run(pg, t, bits, 0, keys, vals)
+    oko, _, _ = o.bulk(oracle.BOP_INSERT, keys, vals)
+    assert ok.all() and oko.all()
+    f, v, _ = _run(pg, t, bits, 1, keys)
+    assert f.all(), "false negatives"
+    # a remove takes the first slot holding the key's tag, which with short
+    # tags is sometimes another key's: both runs remove (almost) every key
+    r, _, _ = _run(pg, t, bits, 2, keys[: n // 2])
+    ro, _, _ = o.bulk(oracle.BOP_REMOVE, keys[: n // 2])
+    assert abs(int(r.sum()) - int(ro.sum())) <= 5 and r.mean() > 0.99
+    occ, tomb = t.get_fill(0)
+    occ1, tomb1 = t.get_fill(1)
+    assert (occ - tomb) + (occ1 - tomb1) == n - int(r.sum())
+    assert o.count_fill(0) + o.count_fill(1) == n - int(ro.sum())
+    a, _, _ = _run(pg, t, bits, 3, keys[: n // 2], vals[: n // 2])
+    assert a.all()
+    occ, tomb = t.get_fill(0)
+    occ1, tomb1 = t.get_fill(1)
+    assert (occ - tomb) + (occ1 - tomb1) == n - int(r.sum()) + n // 2
+
+
+def _ref_stats():
+    p = GOLDEN / "ref_bucketed_stats.json"
+    return json.loads(p.read_text()) if p.exists() else None
+
+
+@pytest.mark.parametrize("name,bits", [("del_tcf", 16), ("del_tcf_small", 8)])
+def test_delete_flow_matches_reference_statistics(pg, name, bits):
+    """The reference's delete test (tests/src/delete_tests.cu:568-760) at 2^22
+    primary slots + 1% backing, 0.9 load, parallel launches.  Zero insert
+    failures, as the reference's run.  A remove takes the first slot holding
+    the key's tag, sometimes another key's, so failed removes, false negatives
+    and failed re-adds may occur in either library: each within 10 of the
+    reference's count; tag-collision value mismatches within 25% (+20) of the
+    reference's (which key a shared tag answers for depends on the order)."""
+    stats = _ref_stats()
+    n0 = 1 << 22
+    n1 = n0 // 100
+    n = int(0.9 * (n0 + n1))
+    mask = (1 << bits) - 1
+    keys = wl.keys_without_sentinels(42, n)
+    vals = wl.values_for(keys, 2, 49).astype(np.uint64) & np.uint64(mask)
+    t = pg.Table(pg.data_structs.del_tcf(n0, n1, tag_bits=bits), 42)
+    half = n // 2
+    ok, _, _ = _run(pg, t, bits, 0, keys, vals)
+    r, _, _ = _run(pg, t, bits, 2, keys[:half])
+    qf, qv, _ = _run(pg, t, bits, 1, keys[half:])
+    a, _, _ = _run(pg, t, bits, 3, keys[:half], vals[:half])
+    af, _, _ = _run(pg, t, bits, 1, keys)
+    mism = int((qf & (qv != vals[half:])).sum())
+    fn = int((~qf & ok[half:]).sum())
+    assert (~ok).sum() == 0
+    assert (~r).sum() <= 10 and fn <= 10 and (~a).sum() <= 10 and (~af).sum() <= 20
+    if stats is not None:
+        ref = stats[name]
+        assert ref["insert_failures"] == 0
+        assert abs(int((~r).sum()) - ref["remove_misses"]) <= 10
+        assert abs(fn - ref["query_misses"]) <= 10
+        assert abs(int((~a).sum()) - ref["readd_failures"]) <= 10
+        assert abs(mism - ref["query_value_mismatches"]) <= 0.25 * ref["query_value_mismatches"] + 20
+
+
+def test_insert_if_not_exists_reports_present_keys(pg):
+    import torch
+    t = pg.Table(pg.data_structs.del_tcf(1 << 16, 1 << 10), 5)
+    keys = wl.keys_without_sentinels(8, 40000)
+    vals = wl.values_for(keys, 2, 4).astype(np.uint64) & np.uint64(0xFFFF)
+    ok, _, _ = _run(pg, t, 16, 0, keys[:20000], vals[:20000])
+    assert ok.all()
+    ok2, out, fd = _run(pg, t, 16, 4, keys, (vals + 1) & np.uint64(0xFFFF))
+    assert ok2.all() and fd[:20000].all()
+    # a present key reports a stored value of its tag (its own unless a tag collides)
+    assert (out[:20000] == vals[:20000]).mean() > 0.99
+    # absent keys were inserted unless a colliding tag already answered for them
+    assert fd[20000:].mean() < 0.05
+    f, _, _ = _run(pg, t, 16, 1, keys)
+    assert f.all()
+    # the _delete form removes what it finds
+    ok3, _, fd3 = _run(pg, t, 16, 5, keys[:1000], vals[:1000])
+    assert ok3.all() and fd3.all()
+    occ, tomb = t.get_fill(0)
+    assert tomb >= 900
+    del torch
+
+
+def test_packed_formats_reject_unsupported_calls(pg):
+    import torch
+    t = pg.Table(pg.data_structs.hash_table_64(1 << 12, bucket=8), 1)
+    k = to_dev(wl.keys_without_sentinels(1, 10))
+    with pytest.raises(pg.PoggersError):
+        t.bulk_insert_with_delete(k)
+    with pytest.raises(pg.PoggersError):
+        pg.Batch([pg.Table(pg.data_structs.del_tcf(1 << 12, 64), 1)], 16)
+    del torch
