@@ -3,6 +3,7 @@
     python -m poggers_b200.bench_configs --config 1   # plain TCF, 2^22 slots
     python -m poggers_b200.bench_configs --config 3   # 1024 TCFs: batched vs per-table launches
     python -m poggers_b200.bench_configs --config 4   # served request stream vs plain per-request path
+    python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots), ours vs reference
 
 Each prints one JSON line.  All inputs are seeded synthetic keys.
 """
@@ -287,6 +288,95 @@ def config4(args):
             "plain_requests": args.plain_requests}
 
 
+# ---------------------------------------------------------------- delete flow
+def config_del(args):
+    """The reference's delete test (tests/src/delete_tests.cu:568-760) on the
+    bucketed filter with tombstone reuse: 2^log2 primary slots + 1% backing,
+    16-bit tags; insert 0.9 of the slots, remove the first half, query the
+    second half, re-add the first half with insert_with_delete.  Each phase is
+    timed with CUDA events, for this library and (when its build is present)
+    for the reference's own CUDA build on the same GPU, same keys."""
+    import torch
+    n0 = 1 << args.log2
+    n1 = n0 // 100
+    n = int(0.9 * (n0 + n1))
+    half = n // 2
+    keys = wl.keys_without_sentinels(42, n)
+    vals = (wl.values_for(keys, 2, 49).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    dv = torch.from_numpy(vals.view(np.int16)).cuda()
+    dk1, dk2, dv1 = dk[:half].contiguous(), dk[half:].contiguous(), dv[:half].contiguous()
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    qv = torch.zeros(n - half, dtype=torch.int16, device="cuda")
+
+    def phases(run):
+        e = _events(5)
+        e[0].record()
+        run(0, dk, dv, ok)
+        e[1].record()
+        run(2, dk1, None, ok[:half])
+        e[2].record()
+        run(1, dk2, None, ok[half:], qv)
+        e[3].record()
+        run(3, dk1, dv1, ok[:half])
+        e[4].record()
+        torch.cuda.synchronize()
+        return [e[i].elapsed_time(e[i + 1]) for i in range(4)]
+
+    def summarize(ms):
+        med = np.median(np.array(ms), axis=0)
+        units = [n, half, n - half, half]
+        names = ["insert", "remove", "query", "insert_with_delete"]
+        out = {f"{k}_mops": round(u / m / 1e3, 1) for k, u, m in zip(names, units, med)}
+        out["total_mops"] = round(sum(units) / med.sum() / 1e3, 1)
+        out["ms"] = [round(float(x), 3) for x in med]
+        return out
+
+    res = {"config": "del", "workload": f"bucketed filter, 16-bit tags: 2^{args.log2} slots (16/bucket) + 1% "
+                                       f"backing (8/bucket, linear), 0.9 load; insert, remove 1/2, query 1/2, "
+                                       f"re-add 1/2", "keys": n}
+    for lanes in (1, 4):
+        t = pg.Table(pg.data_structs.del_tcf(n0, n1), 42)
+        t.set_launch(256, 32, 0, lanes)
+
+        def run(op, k, v, fl, out=None):
+            if op == 0:
+                t.bulk_insert(k, v, fl)
+            elif op == 1:
+                t.bulk_query(k, out, fl)
+            elif op == 2:
+                t.bulk_remove(k, fl)
+            else:
+                t.bulk_insert_with_delete(k, v, fl)
+
+        ms = []
+        for step in range(args.steps + 2):
+            t.clear()
+            m = phases(run)
+            if step >= 2:
+                ms.append(m)
+        res[f"ours_lanes{lanes}"] = summarize(ms)
+        del t
+    try:
+        from oracle import pyrefcuda as rc
+        if rc.available():
+            ms = []
+            for step in range(args.steps + 2):
+                r = rc.RefTable(rc.KIND_DEL_TCF, n0, n1, 42)
+
+                def rrun(op, k, v, fl, out=None):
+                    r.bbulk(op if op != 3 else rc.OP_INSERT_DELETE, k, v, fl, out)
+
+                m = phases(rrun)
+                r.close()
+                if step >= 2:
+                    ms.append(m)
+            res["reference_cuda"] = summarize(ms)
+    except (ImportError, RuntimeError) as e:
+        res["reference_cuda"] = f"unavailable: {e}"
+    return res
+
+
 def srv_config_of(kind, n):
     if kind == "ht":
         cfg = pg.data_structs.hash_table_64(n, bucket=8)
@@ -297,7 +387,8 @@ def srv_config_of(kind, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", type=int, required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "del"], required=True)
+    ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--tables", type=int, default=1024)
     ap.add_argument("--bucket", type=int, default=16)
@@ -310,7 +401,7 @@ def main():
     a = ap.parse_args()
     import torch
     torch.cuda.init()
-    fn = {1: config1, 3: config3, 4: config4}[a.config]
+    fn = {"1": config1, "3": config3, "4": config4, "del": config_del}[a.config]
     print(json.dumps(fn(a)))
 
 

@@ -254,7 +254,9 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
     t->block_threads = 256;
     t->blocks_per_sm = 32;
     t->max_blocks = 0;
-    t->lanes = cfg->tile;
+    // packed buckets: one lane reads a whole 64-byte bucket in one go and measured
+    // fastest (the lanes never change a result); otherwise the config's tile
+    t->lanes = packed(cfg->format) ? 1u : cfg->tile;
     t->partition = 1;
     t->ifmt = internal_format(cfg);
     t->desc.nlevels = cfg->nlevels;
