@@ -4,10 +4,139 @@
 
 namespace pg {
 
+// Query with lane refill.  A negative query walks a variable number of
+// buckets (1 to max_probes), and with one key per lane a warp would run as
+// long as its slowest lane while the others idle.  Here every warp owns a
+// contiguous range of the batch and runs probe steps: in each step every
+// active lane does one bucket of its key, and a lane whose key is resolved
+// takes the next key of the warp's range, so the warp's lanes stay busy until
+// the range is exhausted.  The per-key rule is level_ops_fp::query_s exactly
+// (first fingerprint match at or before the first empty slot of a bucket,
+// a bucket with an empty slot ends the walk); a primary miss goes to the
+// backing level.
+template <int B, bool BK>
+__global__ void __launch_bounds__(256) k_query_fp_refill(table_desc t, bulk_args a)
+{
+    using P = level_ops_fp<B>;
+    using BKO = backing_ops<FMT_KV64, 1>;
+    constexpr int NW = P::NW;
+    const level_desc &L = t.lv[0];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t per = (a.n + nwarps - 1) / nwarps;
+    uint64_t cursor = warp * per;
+    const uint64_t end = cursor + per < a.n ? cursor + per : a.n;
+    const uint64_t keep = l2_policy_evict_last(), stream = l2_policy_evict_first();
+    unsigned long long *vout = static_cast<unsigned long long *>(a.vals_out);
+    const uint32_t lt = (1u << lane) - 1u;
+    bool active = false;
+    uint64_t idx = 0, key = 0;
+    uint32_t f = 0, i = 0;
+    probe_seq ps;
+    uint32_t hits = 0;
+    while (true) {
+        // refill: lanes without a key take the next keys of the range, in lane order
+        const uint32_t need = __ballot_sync(0xffffffffu, !active);
+        if (need) {
+            const uint64_t mine = cursor + __popc(need & lt);
+            cursor += __popc(need);
+            if (!active && mine < end) {
+                active = true;
+                idx = mine;
+                key = __ldcs(a.keys + idx);
+                ps.begin(L.probe, key, key, L.seed, L.seed2);
+                f = fp_of(key, ps.h1);
+                i = 0;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            // one bucket of this lane's key
+            bool done = false, hit = false;
+            unsigned long long v = 0;
+            const uint64_t raw = ps.at(i);
+            if (raw == kProbeEnd) {
+                done = true;
+            } else {
+                const uint64_t b = L.nbmod.mod(raw);
+                uint32_t w[NW];
+                P::load_fp(L, b, w, keep);
+                const uint32_t e = P::match(w, 0);
+                uint32_t cand = P::match(w, f) & P::upto(e);
+                while (cand) {
+                    const int sl = __ffs(cand) - 1;
+                    unsigned long long k, vv;
+                    P::load_slot(L, b, sl, k, vv, stream);
+                    if (k == key) {
+                        hit = true;
+                        v = vv;
+                        break;
+                    }
+                    cand &= cand - 1;
+                }
+                done = hit || e != 0 || ++i >= L.max_probes;
+            }
+            if (done) {
+                if (!hit && BK && t.nlevels > 1) {
+                    const group<1> g1 = group<1>::make();
+                    hit = BKO::query(t.lv[1], g1, key, &v);
+                }
+                if (vout) __stcs(vout + idx, hit ? v : 0ULL);
+                if (a.flags) __stcs(a.flags + idx, (uint8_t)hit);
+                hits += hit;
+                active = false;
+            }
+        }
+    }
+    add_count(a.count, hits);
+}
+
+// resident 256-thread blocks of a kernel on the current device (0 if unknown);
+// looked up once per kernel
+int refill_blocks(const void *fn)
+{
+    static const void *keys[8];
+    static int vals[8];
+    for (int k = 0; k < 8; ++k)
+        if (keys[k] == fn) return vals[k];
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm <= 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int k = 0; k < 8; ++k)
+        if (!keys[k]) {
+            vals[k] = sms * per_sm;
+            keys[k] = fn;
+            break;
+        }
+    return sms * per_sm;
+}
+
+template <int B, bool BK>
+cudaError_t launch_query_refill(const table_desc &t, const bulk_args &a, dim3 grid, cudaStream_t s)
+{
+    const void *fn = (const void *)k_query_fp_refill<B, BK>;
+    const int blocks = refill_blocks(fn);
+    // one resident wave of blocks, never more warps than keys
+    uint64_t g = blocks > 0 ? (uint64_t)blocks : grid.x;
+    const uint64_t max_by_keys = (a.n + 255) / 256;
+    if (g > max_by_keys) g = max_by_keys;
+    if (g < 1) g = 1;
+    k_query_fp_refill<B, BK><<<(unsigned)g, 256, 0, s>>>(t, a);
+    return cudaGetLastError();
+}
+
 template <int B>
 cudaError_t launch_fp_b(int op, const table_desc &t, const bulk_args &a, dim3 grid, dim3 block, cudaStream_t s)
 {
     const bool bk = t.nlevels > 1;
+    // the refill query needs whole warps; the serial shape (one lane) keeps the plain kernel
+    if (op == OP_QUERY && block.x == 256 && grid.x > 1)
+        return bk ? launch_query_refill<B, true>(t, a, grid, s) : launch_query_refill<B, false>(t, a, grid, s);
     return bk ? launch_bgs<FMT_KV64_FP, B, 1, SCHEME_BUCKET, true>(op, t, a, grid, block, s)
               : launch_bgs<FMT_KV64_FP, B, 1, SCHEME_BUCKET, false>(op, t, a, grid, block, s);
 }

@@ -330,3 +330,26 @@ def test_layouts_match_oracle(pg, oracle, layout, tile, bucket):
     both[-2:] = False
     assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
     assert t.get_fill(0)[1] == int(ok[ridx].sum())
+
+
+def test_fingerprints_with_backing_level_matches_oracle(pg, oracle):
+    """A fingerprinted primary over a backing level: keys that overflow the
+    primary land in the backing table, and every query (the lane-refill query
+    kernel included) agrees with the oracle on keys both runs placed."""
+    levels = [(1 << 16, 8, 3, 0, 0), (1 << 14, 8, 20, 0, 0)]
+    cfg = pg.TableConfig(pg.FMT_KV64, 4, [pg.Level(*lv) for lv in levels])
+    cfg.fingerprints = True
+    t = pg.Table(cfg, 9)
+    d = Driver(t)
+    o = oracle.OracleTable(0, 4, levels, 9)
+    n = (1 << 16) + (1 << 13)
+    keys = wl.keys_without_sentinels(31, n)
+    vals = wl.values_for(keys, 8, 32)
+    q = np.concatenate([keys, wl.keys_without_sentinels(33, 20000)])
+    ok, oko = d.insert(keys, vals), o.insert_many(keys, vals)
+    assert t.get_fill(1)[0] > 1000, "the backing level was not used"
+    both = np.concatenate([ok & oko, np.ones(20000, dtype=bool)])
+    f, v = d.query(q)
+    fo, vo = o.query_many(q)
+    assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
+    assert (f[:n] == ok).all()
