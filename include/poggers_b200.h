@@ -218,6 +218,19 @@ pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_s
 pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst, uint64_t bytes);
 pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes);
 
+/* Checkpoint image of a whole table, for save / restore of resident tables
+ * (no counterpart in the reference, which has no on-disk form).  Layout,
+ * little-endian: a 128-byte header (magic "PGB2TBL1", version 1, header
+ * size, the pg_table_config, the seed, each level's byte count, an FNV-1a
+ * 64 checksum of the payload), then every level in the reference's slot
+ * layout (pg_table_dump_level).  Synchronous. */
+#define PG_IMAGE_HEADER_BYTES 128
+uint64_t pg_table_image_bytes(const pg_table *t);
+pg_status pg_table_save_image(const pg_table *t, void *host_dst, uint64_t bytes);
+/* Create a table on the current device from an image.  A short, corrupt or
+ * foreign image returns PG_ERR_INVALID before anything is allocated. */
+pg_status pg_table_load_image(const void *host_src, uint64_t bytes, pg_table **out);
+
 /* ---------------------------------------------------------------------------
  * Multi-table batches: many requests over many tables in one persistent launch.
  *

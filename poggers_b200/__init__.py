@@ -83,6 +83,7 @@ EXPORTED = (
     "pg_bulk_insert", "pg_bulk_insert_with_delete", "pg_bulk_insert_if_not_exists",
     "pg_bulk_insert_if_not_exists_delete", "pg_bulk_query",
     "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
+    "pg_table_image_bytes", "pg_table_save_image", "pg_table_load_image",
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
@@ -131,6 +132,12 @@ def lib() -> C.CDLL:
         getattr(L, f).argtypes = [V, P, P, U64, P, P, P, P, P]
     L.pg_bulk_remove.restype = C.c_int
     L.pg_bulk_remove.argtypes = [V, P, U64, P, P, P]
+    L.pg_table_image_bytes.restype = U64
+    L.pg_table_image_bytes.argtypes = [V]
+    L.pg_table_save_image.restype = C.c_int
+    L.pg_table_save_image.argtypes = [V, C.c_void_p, U64]
+    L.pg_table_load_image.restype = C.c_int
+    L.pg_table_load_image.argtypes = [C.c_void_p, U64, C.POINTER(V)]
     L.pg_table_count_fill.restype = C.c_int
     L.pg_table_count_fill.argtypes = [V, U32, P, P]
     L.pg_table_dump_level.restype = C.c_int
@@ -389,9 +396,43 @@ class Table:
         _check(lib().pg_table_dump_level(self._h, level, buf, nbytes), "pg_table_dump_level")
         return buf.raw
 
+    def save_image(self) -> bytes:
+        """Checkpoint image: header + every level in the reference's slot layout."""
+        n = lib().pg_table_image_bytes(self._h)
+        buf = C.create_string_buffer(n)
+        _check(lib().pg_table_save_image(self._h, buf, n), "pg_table_save_image")
+        return buf.raw
+
+    def save(self, path) -> None:
+        Path(path).write_bytes(self.save_image())
+
+    @classmethod
+    def from_image(cls, data: bytes) -> "Table":
+        buf = C.create_string_buffer(bytes(data), len(data))
+        h = C.c_void_p()
+        _check(lib().pg_table_load_image(buf, len(data), C.byref(h)), "pg_table_load_image")
+        t = cls.__new__(cls)
+        t._h = h
+        t.config = _config_from_image(bytes(data))
+        t.seed = int.from_bytes(bytes(data[80:88]), "little")
+        return t
+
+    @classmethod
+    def load(cls, path) -> "Table":
+        return cls.from_image(Path(path).read_bytes())
+
     def load_level(self, level: int, data: bytes) -> None:
         buf = C.create_string_buffer(bytes(data), len(data))
         _check(lib().pg_table_load_level(self._h, level, buf, len(data)), "pg_table_load_level")
+
+
+def _config_from_image(data: bytes) -> TableConfig:
+    """The TableConfig recorded in a checkpoint image's header."""
+    c = _TableConfig.from_buffer_copy(data[16:16 + C.sizeof(_TableConfig)])
+    levels = [Level(c.levels[i].nslots, c.levels[i].bucket_size, c.levels[i].max_probes, c.levels[i].scheme,
+                    c.levels[i].probe) for i in range(c.nlevels)]
+    return TableConfig(c.format, c.tile, levels, bool(c.flags & PG_TABLE_SPLIT_BUCKETS),
+                       bool(c.flags & PG_TABLE_FINGERPRINTS))
 
 
 # ---------------------------------------------------------------- named tables

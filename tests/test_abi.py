@@ -100,3 +100,34 @@ def test_probe_buckets_match_oracle(pg, oracle, name):
             ref = [v % nb for v in oracle.probe_values(L.probe, s, fmt, k, L.max_probes)]
             assert mine == ref
         s = (s * s) % (1 << 64)
+
+
+def test_load_image_rejects_bad_images_before_touching_the_gpu(pg):
+    """A short, foreign or corrupt checkpoint image is refused by the header
+    and checksum checks, before any device allocation."""
+    lib = pg.lib()
+    h = C.c_void_p()
+    assert lib.pg_table_load_image(None, 0, C.byref(h)) == pg.PG_ERR_INVALID
+    short = C.create_string_buffer(64)
+    assert lib.pg_table_load_image(short, 64, C.byref(h)) == pg.PG_ERR_INVALID
+    # a well-formed header whose payload checksum does not match
+    hdr = bytearray(128)
+    hdr[0:8] = b"PGB2TBL1"
+    hdr[8:12] = (1).to_bytes(4, "little")
+    hdr[12:16] = (128).to_bytes(4, "little")
+    cfg = pg.data_structs.hash_table_64(64, bucket=8).c()
+    hdr[16:80] = bytes(cfg)
+    hdr[88:96] = (64 * 16).to_bytes(8, "little")
+    hdr[104:112] = (12345).to_bytes(8, "little")
+    img = bytes(hdr) + bytes(64 * 16)
+    buf = C.create_string_buffer(img, len(img))
+    assert lib.pg_table_load_image(buf, len(img), C.byref(h)) == pg.PG_ERR_INVALID
+    # wrong magic
+    bad = bytearray(img)
+    bad[0] = ord("X")
+    buf = C.create_string_buffer(bytes(bad), len(bad))
+    assert lib.pg_table_load_image(buf, len(bad), C.byref(h)) == pg.PG_ERR_INVALID
+    # payload size disagreeing with the header
+    buf = C.create_string_buffer(img[:-16], len(img) - 16)
+    assert lib.pg_table_load_image(buf, len(img) - 16, C.byref(h)) == pg.PG_ERR_INVALID
+    assert not h.value
