@@ -158,6 +158,29 @@ uint64_t pg_table_bytes(const pg_table *t);
 pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
                               uint32_t lanes_per_key);
 
+/* ---------------------------------------------------------------------------
+ * One logical table partitioned over several GPUs (no counterpart in the
+ * reference, whose tables live on one GPU).  Key k belongs to shard
+ * pg_host_shard_of(k, route_seed, nshards) = high bits of
+ * MurmurHash64A(k, route_seed) * nshards; each GPU holds its shard as an
+ * ordinary table.  A bulk call routes its batch (pg_route_by_shard), the
+ * caller exchanges the per-shard runs with an all-to-all (NCCL), each GPU
+ * runs the bulk operation on what it received, the results travel back by
+ * the reverse all-to-all and pg_scatter_by_perm puts them in batch order
+ * (poggers_b200/sharded.py does all of this over torch.distributed). */
+uint32_t pg_host_shard_of(uint64_t key, uint64_t route_seed, uint32_t nshards);
+/* Counting sort of n < 2^32 keys (and values of val_bytes 0, 1, 2 or 8) by
+ * shard: d_keys_out / d_vals_out hold the shards' runs in shard order,
+ * d_perm_out[i] = the batch position of output i, d_counts[0..nshards) = run
+ * lengths; d_counts must hold 2 * nshards entries (the second half is
+ * scratch).  nshards <= 1024.  Stream-ordered. */
+pg_status pg_route_by_shard(const uint64_t *d_keys, const void *d_vals, uint32_t val_bytes, uint64_t n,
+                            uint32_t nshards, uint64_t route_seed, uint64_t *d_keys_out, void *d_vals_out,
+                            uint32_t *d_perm_out, uint64_t *d_counts, pg_stream_t stream);
+/* d_dst[d_perm[i]] = d_src[i] for elements of 1, 2 or 8 bytes. */
+pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t n, uint32_t elem_bytes, void *d_dst,
+                             pg_stream_t stream);
+
 /* Region-ordered inserts (on by default; enable = 0 turns them off).  A
  * batch of at least 2^20 keys into a uint64 bucket table of at least 64 MB
  * is first counting-sorted by the table region (32 MB) of each key's first

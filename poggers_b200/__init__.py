@@ -85,6 +85,7 @@ EXPORTED = (
     "pg_bulk_remove", "pg_table_count_fill", "pg_table_dump_level", "pg_table_load_level",
     "pg_table_image_bytes", "pg_table_save_image", "pg_table_load_image",
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
+    "pg_host_shard_of", "pg_route_by_shard", "pg_scatter_by_perm",
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
@@ -132,6 +133,12 @@ def lib() -> C.CDLL:
         getattr(L, f).argtypes = [V, P, P, U64, P, P, P, P, P]
     L.pg_bulk_remove.restype = C.c_int
     L.pg_bulk_remove.argtypes = [V, P, U64, P, P, P]
+    L.pg_host_shard_of.restype = U32
+    L.pg_host_shard_of.argtypes = [U64, U64, U32]
+    L.pg_route_by_shard.restype = C.c_int
+    L.pg_route_by_shard.argtypes = [P, P, U32, U64, U32, U64, P, P, P, P, P]
+    L.pg_scatter_by_perm.restype = C.c_int
+    L.pg_scatter_by_perm.argtypes = [P, P, U64, U32, P, P]
     L.pg_table_image_bytes.restype = U64
     L.pg_table_image_bytes.argtypes = [V]
     L.pg_table_save_image.restype = C.c_int

@@ -35,13 +35,29 @@ constexpr uint64_t kPartRegionBytes = (uint64_t)PG_PART_REGION_MB << 20;  // tab
 constexpr uint64_t kPartMinKeys = 1ull << 20;         // smaller batches insert unsorted
 
 // region of a key = its first bucket >> shift: regions are runs of 2^shift buckets
-__device__ __forceinline__ uint32_t region_of(const level_desc &L, uint64_t key, uint32_t shift)
-{
-    return (uint32_t)(L.nbmod.mod(murmur64a_u64(key, L.seed)) >> shift);
-}
+struct region_router {
+    level_desc L;
+    uint32_t shift;
+    __device__ __forceinline__ uint32_t operator()(uint64_t key) const
+    {
+        return (uint32_t)(L.nbmod.mod(murmur64a_u64(key, L.seed)) >> shift);
+    }
+};
 
-__global__ void __launch_bounds__(kPartThreads) k_part_count(level_desc L, const uint64_t *keys, uint64_t n,
-                                                             uint32_t shift, uint32_t R, unsigned long long *counts)
+// owner of a key among nshards shards: the high bits of a routing hash
+// (multiply-shift, so owners are uniform for any shard count)
+struct shard_router {
+    uint64_t seed;
+    uint32_t nshards;
+    __device__ __forceinline__ uint32_t operator()(uint64_t key) const
+    {
+        return (uint32_t)umulhi64(murmur64a_u64(key, seed), nshards);
+    }
+};
+
+template <class Router>
+__global__ void __launch_bounds__(kPartThreads) k_part_count(Router route, const uint64_t *keys, uint64_t n,
+                                                             uint32_t R, unsigned long long *counts)
 {
     __shared__ unsigned int hist[kPartMaxRegions];
     for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) hist[r] = 0;
@@ -57,7 +73,7 @@ __global__ void __launch_bounds__(kPartThreads) k_part_count(level_desc L, const
         }
 #pragma unroll
         for (uint32_t j = 0; j < kPartPerThread; j++)
-            if (i0 + j * stride < n) atomicAdd(&hist[region_of(L, k[j], shift)], 1u);
+            if (i0 + j * stride < n) atomicAdd(&hist[route(k[j])], 1u);
     }
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < R; r += blockDim.x)
@@ -87,17 +103,16 @@ __global__ void k_part_scan(const unsigned long long *counts, unsigned long long
 // shared memory, reserve one run per region from the global cursors, sort the
 // tile by region in shared memory, then write each region's run with
 // consecutive threads on consecutive addresses.
-__global__ void __launch_bounds__(kPartThreads) k_part_scatter(level_desc L, const uint64_t *keys,
-                                                               const unsigned long long *vals, uint64_t n,
-                                                               uint32_t shift, uint32_t R,
-                                                               unsigned long long *cursors, uint64_t *okeys,
-                                                               unsigned long long *ovals, uint32_t *operm)
+template <class Router, class V>
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter(Router route, const uint64_t *keys, const V *vals,
+                                                               uint64_t n, uint32_t R, unsigned long long *cursors,
+                                                               uint64_t *okeys, V *ovals, uint32_t *operm)
 {
     __shared__ unsigned long long gbase[kPartMaxRegions];
     __shared__ unsigned int cnt[kPartMaxRegions];
     __shared__ unsigned int lstart[kPartMaxRegions];
     __shared__ uint64_t sk[kPartTile];
-    __shared__ unsigned long long sv[kPartTile];
+    __shared__ V sv[kPartTile];
     __shared__ uint32_t sp[kPartTile];
     __shared__ uint16_t sr[kPartTile];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -106,14 +121,14 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(level_desc L, con
         for (uint32_t r = tid; r < R; r += blockDim.x) cnt[r] = 0;
         __syncthreads();
         uint64_t k[kPartPerThread];
-        unsigned long long v[kPartPerThread];
+        V v[kPartPerThread];
         uint32_t reg[kPartPerThread], rank[kPartPerThread];
 #pragma unroll
         for (uint32_t j = 0; j < kPartPerThread; j++) {
             const uint32_t e = j * kPartThreads + tid;
             if (e < tn) {
                 k[j] = __ldcs(keys + t0 + e);
-                v[j] = ovals ? __ldcs(vals + t0 + e) : 0ULL;
+                v[j] = ovals ? vals[t0 + e] : (V)0;
             }
         }
 #pragma unroll
@@ -121,7 +136,7 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(level_desc L, con
             const uint32_t e = j * kPartThreads + tid;
             reg[j] = 0xFFFFFFFFu;
             if (e < tn) {
-                reg[j] = region_of(L, k[j], shift);
+                reg[j] = route(k[j]);
                 rank[j] = atomicAdd(&cnt[reg[j]], 1u);
             }
         }
@@ -212,13 +227,112 @@ bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
     const level_desc &L = t->desc.lv[0];
     const unsigned grid = (unsigned)(t->num_sms * 8);
     cudaMemsetAsync(counts, 0, R * 8, s);
-    k_part_count<<<grid, kPartThreads, 0, s>>>(L, a.keys, n, shift, R, counts);
+    const region_router route{L, shift};
+    k_part_count<<<grid, kPartThreads, 0, s>>>(route, a.keys, n, R, counts);
     k_part_scan<<<1, 32, 0, s>>>(counts, cursors, R);
-    k_part_scatter<<<grid, kPartThreads, 0, s>>>(L, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
-                                                 shift, R, cursors, okeys, ovals, operm);
+    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
+                                                 R, cursors, okeys, ovals, operm);
     if (a.flags) cudaMemsetAsync(a.flags, 1, n, s);
     a.keys = okeys;
     a.vals_in = ovals;
     a.perm = operm;
     return true;
 }
+
+// ---------------------------------------------------------------- sharding
+// Routing of a batch to the shards of a table partitioned over several GPUs:
+// the same counting sort, by owner instead of by region.
+
+namespace pg {
+
+template <class V>
+__global__ void __launch_bounds__(256) k_scatter_by_perm(const V *src, const uint32_t *perm, uint64_t n, V *dst)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[perm[i]] = src[i];
+}
+
+namespace {
+
+template <class V>
+pg_status route_t(const uint64_t *keys, const void *vals, uint64_t n, uint32_t nshards, uint64_t seed,
+                  uint64_t *okeys, void *ovals, uint32_t *operm, uint64_t *counts, cudaStream_t s, unsigned grid)
+{
+    const shard_router route{seed, nshards};
+    unsigned long long *c = reinterpret_cast<unsigned long long *>(counts);
+    unsigned long long *cur = c + nshards;
+    if (cudaMemsetAsync(c, 0, nshards * sizeof(unsigned long long), s) != cudaSuccess) return PG_ERR_CUDA;
+    k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, nshards, c);
+    k_part_scan<<<1, 32, 0, s>>>(c, cur, nshards);
+    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const V *>(vals), n, nshards, cur, okeys,
+                                                 static_cast<V *>(ovals), operm);
+    return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 148;
+    }
+    return sms;
+}
+
+}  // namespace
+
+}  // namespace pg
+
+extern "C" {
+
+uint32_t pg_host_shard_of(uint64_t key, uint64_t route_seed, uint32_t nshards)
+{
+    if (nshards == 0) return 0;
+    return (uint32_t)pg::umulhi64(pg::murmur64a_u64(key, route_seed), nshards);
+}
+
+pg_status pg_route_by_shard(const uint64_t *d_keys, const void *d_vals, uint32_t val_bytes, uint64_t n,
+                            uint32_t nshards, uint64_t route_seed, uint64_t *d_keys_out, void *d_vals_out,
+                            uint32_t *d_perm_out, uint64_t *d_counts, pg_stream_t stream)
+{
+    if (nshards == 0 || nshards > pg::kPartMaxRegions || !d_counts) return PG_ERR_INVALID;
+    if (n >= (1ull << 32)) return PG_ERR_INVALID;
+    if (!(val_bytes == 0 || val_bytes == 1 || val_bytes == 2 || val_bytes == 8)) return PG_ERR_INVALID;
+    if (val_bytes && (!d_vals) != (!d_vals_out)) return PG_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        return cudaMemsetAsync(d_counts, 0, nshards * sizeof(uint64_t), s) == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+    }
+    if (!d_keys || !d_keys_out || !d_perm_out) return PG_ERR_INVALID;
+    const unsigned grid = (unsigned)(pg::sm_count() * 8);
+    const void *v = val_bytes ? d_vals : nullptr;
+    void *vo = val_bytes ? d_vals_out : nullptr;
+    switch (val_bytes) {
+    case 8: return pg::route_t<unsigned long long>(d_keys, v, n, nshards, route_seed, d_keys_out, vo, d_perm_out,
+                                                   d_counts, s, grid);
+    case 2: return pg::route_t<unsigned short>(d_keys, v, n, nshards, route_seed, d_keys_out, vo, d_perm_out,
+                                               d_counts, s, grid);
+    case 1: return pg::route_t<unsigned char>(d_keys, v, n, nshards, route_seed, d_keys_out, vo, d_perm_out,
+                                              d_counts, s, grid);
+    default: return pg::route_t<unsigned long long>(d_keys, nullptr, n, nshards, route_seed, d_keys_out, nullptr,
+                                                    d_perm_out, d_counts, s, grid);
+    }
+}
+
+pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t n, uint32_t elem_bytes, void *d_dst,
+                             pg_stream_t stream)
+{
+    if (n == 0) return PG_OK;
+    if (!d_src || !d_perm || !d_dst) return PG_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const unsigned grid = (unsigned)(pg::sm_count() * 8);
+    switch (elem_bytes) {
+    case 1: pg::k_scatter_by_perm<unsigned char><<<grid, 256, 0, s>>>(static_cast<const unsigned char *>(d_src), d_perm, n, static_cast<unsigned char *>(d_dst)); break;
+    case 2: pg::k_scatter_by_perm<unsigned short><<<grid, 256, 0, s>>>(static_cast<const unsigned short *>(d_src), d_perm, n, static_cast<unsigned short *>(d_dst)); break;
+    case 8: pg::k_scatter_by_perm<unsigned long long><<<grid, 256, 0, s>>>(static_cast<const unsigned long long *>(d_src), d_perm, n, static_cast<unsigned long long *>(d_dst)); break;
+    default: return PG_ERR_INVALID;
+    }
+    return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
+
+}  // extern "C"
