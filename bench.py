@@ -227,7 +227,7 @@ def run_ours(args, rank, world):
                               "block_threads": BLOCK_THREADS, "blocks_per_sm": BLOCKS_PER_SM,
                               "bucket_layout": args.layout, "insert_order": args.insert_order},
                    "parallelism": f"independent table per GPU x{world}",
-                   "l2": "inputs larger than L2 (1 GiB table, 126 MB L2)"},
+                   "l2": f"inputs larger than L2 ({NSLOTS * 16 >> 20} MiB table, 126 MB L2)"},
         "roofline": {"bound": "hbm", "kernel": f"bulk_{dom}", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic, "algo_bytes_per_op": ALGO_BYTES[dom], "units_per_launch": dom_units},
@@ -444,7 +444,8 @@ def allreduce_max(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -157,3 +157,44 @@ def test_owner_function_is_uniform_and_matches_host_helper():
     k = int(keys[0])
     h = pg.lib().pg_host_murmur64a(k, ROUTE_SEED)
     assert pg.lib().pg_host_shard_of(k, ROUTE_SEED, 8) == (h * 8) >> 64
+
+
+def _bench_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+        import bench
+        bench.barrier(world)
+        m = bench.allreduce_max(10.0 + rank, world)
+        q.put((rank, "ok" if m == 10.0 + world - 1 else f"max {m}"))
+    except Exception as ex:
+        q.put((rank, f"{type(ex).__name__}: {ex}"))
+    finally:
+        if dist.is_initialized():
+            dist.destroy_process_group()
+
+
+def test_bench_rank_timing_helpers_over_gloo():
+    """bench.py's multi-rank timing takes the max over ranks of the device time."""
+    import queue
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = {}
+    for _ in range(2):
+        try:
+            r, msg = q.get(timeout=120)
+        except queue.Empty:
+            break
+        results[r] = msg
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert results == {0: "ok", 1: "ok"}, results
