@@ -4,6 +4,7 @@
     python -m poggers_b200.bench_configs --config 3   # 1024 TCFs: batched vs per-table launches
     python -m poggers_b200.bench_configs --config 4   # served request stream vs plain per-request path
     python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots), ours vs reference
+    python -m poggers_b200.bench_configs --config 5   # large: 2^30-slot HT, 2^32-slot tag-only TCF, slab churn, served HT
 
 Each prints one JSON line.  All inputs are seeded synthetic keys.
 """
@@ -377,6 +378,182 @@ def config_del(args):
     return res
 
 
+# ---------------------------------------------------------------- config 5
+def _timed(fn):
+    import torch
+    e = _events(2)
+    e[0].record()
+    r = fn()
+    e[1].record()
+    torch.cuda.synchronize()
+    return e[0].elapsed_time(e[1]), r
+
+
+def _zipf_queries(seed, n_inserted, count, a=1.1, qseed=7):
+    """Half Zipf(a)-ranked keys of the inserted stream, half never-inserted keys
+    (interleaved), generated on the device."""
+    import torch
+    npos, nneg = (count + 1) // 2, count // 2  # even positions positive, odd positions absent
+    ranks = wl.device_zipf_ranks(n_inserted, npos, a, qseed)
+    q = torch.empty(count, dtype=torch.int64, device="cuda")
+    q[0::2] = _splitmix_at(seed, ranks)
+    del ranks
+    q[1::2] = wl.device_splitmix64(seed ^ 0x5A5A5A5A, nneg, 0)
+    return q
+
+
+def _splitmix_at(seed, idx):
+    """splitmix64(seed) at the given int64 indices (device)."""
+    import torch
+
+    def lsr(x, s):
+        return torch.bitwise_right_shift(x, s) & ((1 << (64 - s)) - 1)
+
+    z = (idx + 1) * wl._s64(int(wl.GAMMA)) + wl._s64(seed)
+    z = (z ^ lsr(z, 30)) * wl._s64(int(wl.M1))
+    z = (z ^ lsr(z, 27)) * wl._s64(int(wl.M2))
+    z = z ^ lsr(z, 31)
+    z = torch.where(z == 0, torch.ones_like(z), z)
+    return torch.where(z == -1, torch.full_like(z, -2), z)
+
+
+def config5(args):
+    """Large workloads: a 2^30-slot uint64 table (16 GiB + 1 GiB fingerprints) and
+    a 2^32-slot tag-only TCF (8 GiB), each filled to 0.9 and queried with as many
+    Zipf(1.1) keys (half inserted, half absent); slab churn over 2^24
+    allocations of log-uniform sizes in [16, 4096] B (9 power-of-two classes):
+    malloc all, free a seeded random half, malloc it again; and a 2^28-slot
+    uint64 table filled and queried through the serving loop in 2^22-key
+    requests.  Plain launches are timed with CUDA events; the served path by
+    the host clock around submit / poll."""
+    import torch
+    res = {"config": 5}
+    # ---- uint64 table, 2^30 slots
+    ns = 1 << 30
+    n = int(0.9 * ns)
+    cfg = pg.data_structs.hash_table_64(ns, bucket=8)
+    cfg.fingerprints = True
+    t = pg.Table(cfg, 43)
+    t.set_launch(256, 32, 0, 1)
+    k = wl.device_splitmix64(43, n)
+    v = wl.device_splitmix64(50, n)
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    ms_ins, _ = _timed(lambda: t.bulk_insert(k, v, ok))
+    fails = int(n - ok.sum().item())
+    del v
+    q = _zipf_queries(43, n, n)
+    del k
+    found = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    qv = torch.zeros(n, dtype=torch.int64, device="cuda")
+    ms_q, _ = _timed(lambda: t.bulk_query(q, qv, found))
+    pos_found = float(found[0::2].float().mean().item())
+    neg_found = float(found[1::2].float().mean().item())
+    res["ht_2p30"] = {"slots": ns, "inserts": n, "insert_ms": round(ms_ins, 2), "insert_mops": round(n / ms_ins / 1e3, 1),
+                      "insert_failures": fails, "queries": n, "query_ms": round(ms_q, 2),
+                      "query_mops": round(n / ms_q / 1e3, 1), "positive_found": pos_found,
+                      "negative_found": neg_found, "table_bytes": t.host_bytes_in_use()}
+    del q, found, qv, ok, t
+    torch.cuda.empty_cache()
+    # ---- tag-only TCF, 2^32 slots, in chunks of 2^28 keys
+    ns = 1 << 32
+    n = int(0.9 * ns)
+    t = pg.Table(pg.data_structs.tcqf(ns), 42)
+    t.set_launch(256, 32, 0, 1)
+    chunk = 1 << 28
+    fails = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ms_ins = 0.0
+    for s0 in range(0, n, chunk):
+        c = min(chunk, n - s0)
+        kk = wl.device_splitmix64(42, c, s0)
+        m, _ = _timed(lambda: t.bulk_insert(kk, None, None, fails))
+        ms_ins += m
+    del kk
+    nq = 1 << 30
+    ms_q = 0.0
+    hits_pos = hits_neg = 0
+    for s0 in range(0, nq, chunk):
+        qq = _zipf_queries(42, n, chunk, qseed=11 + s0)
+        f = torch.zeros(chunk, dtype=torch.uint8, device="cuda")
+        m, _ = _timed(lambda: t.bulk_query(qq, None, f))
+        ms_q += m
+        hits_pos += int(f[0::2].sum().item())
+        hits_neg += int(f[1::2].sum().item())
+    res["tcf_2p32_tag_only"] = {"slots": ns, "inserts": n, "insert_ms": round(ms_ins, 1),
+                                "insert_mops": round(n / ms_ins / 1e3, 1), "insert_failures": int(fails.item()),
+                                "queries": nq, "query_ms": round(ms_q, 1), "query_mops": round(nq / ms_q / 1e3, 1),
+                                "positive_found": hits_pos / (nq // 2), "false_positive_rate": hits_neg / (nq // 2),
+                                "table_bytes": t.host_bytes_in_use()}
+    del qq, f, t
+    torch.cuda.empty_cache()
+    # ---- slab churn
+    rng = np.random.default_rng(5)
+    na = 1 << 24
+    sizes = np.floor(2.0 ** rng.uniform(4, 12, na)).astype(np.uint32)
+    classes = [16 << i for i in range(9)]
+    cls = np.searchsorted(np.array(classes), sizes)
+    counts = np.bincount(cls, minlength=9)
+    allocs = [int(c * 1.05) + 4096 for c in counts]
+    ss = pg.allocators.size_class_set(classes, allocs)
+    d_sizes = torch.from_numpy(sizes.view(np.int32)).cuda()
+    ptrs = torch.zeros(na, dtype=torch.int64, device="cuda")
+    fc = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ms_m, _ = _timed(lambda: ss.bulk_malloc(d_sizes, ptrs, fc))
+    half = torch.from_numpy(wl.fisher_yates_half(na, 77)).cuda()
+    hp = ptrs[half].contiguous()
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ms_f, _ = _timed(lambda: ss.bulk_free(hp, bad))
+    hs = d_sizes[half].contiguous()
+    hp2 = torch.zeros_like(hp)
+    fc2 = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ms_m2, _ = _timed(lambda: ss.bulk_malloc(hs, hp2, fc2))
+    res["slab_churn"] = {"allocations": na, "classes": classes, "malloc_ms": round(ms_m, 2),
+                         "malloc_mops": round(na / ms_m / 1e3, 1), "free_ms": round(ms_f, 2),
+                         "free_mops": round(len(half) / ms_f / 1e3, 1), "remalloc_ms": round(ms_m2, 2),
+                         "remalloc_mops": round(len(half) / ms_m2 / 1e3, 1), "malloc_failures": int(fc.item()),
+                         "free_rejected": int(bad.item()), "remalloc_failures": int(fc2.item()),
+                         "pool_bytes": int(sum(ss.class_report(c)["pool_bytes"] for c in range(9)))}
+    del ss, ptrs, hp, hp2
+    torch.cuda.empty_cache()
+    # ---- served: 2^28-slot uint64 table through the serving loop
+    ns = 1 << 28
+    n = int(0.9 * ns)
+    req = 1 << 22
+    srv = pg.Server(hbm_budget_bytes=40 << 30, max_wave_keys=1 << 22, max_wave_requests=64)
+    scfg = pg.data_structs.hash_table_64(ns, bucket=8)
+    scfg.fingerprints = True
+    tid = srv.add_table(scfg, 44)
+    keys = wl.splitmix64(44, n)
+    vals = wl.values_for(keys, 8, 45)
+    t0 = time.perf_counter()
+    rids = [srv.submit(tid, pg.PG_OP_INSERT, keys[s:s + req], vals[s:s + req]) for s in range(0, n, req)]
+    lat_i = [srv.poll(r, wait=True)[1] for r in rids]
+    el_i = time.perf_counter() - t0
+    rng = np.random.default_rng(9)
+    ranks = np.minimum(rng.zipf(1.1, n // 2), n) - 1
+    qk = np.empty(n, dtype=np.uint64)
+    qk[0::2][: n // 2] = keys[ranks]
+    qk[1::2][: n - n // 2] = wl.splitmix64(99, n - n // 2)
+    outs = []
+    t0 = time.perf_counter()
+    rids = []
+    for s in range(0, n, req):
+        vo = np.zeros(min(req, n - s), dtype=np.uint64)
+        rids.append(srv.submit(tid, pg.PG_OP_QUERY, qk[s:s + req], None, vo))
+        outs.append(vo)
+    lat_q = [srv.poll(r, wait=True)[1] for r in rids]
+    el_q = time.perf_counter() - t0
+    srv.close()
+    res["served_ht_2p28"] = {"slots": ns, "request_keys": req, "inserts": n,
+                             "insert_mops_e2e": round(n / el_i / 1e6, 1),
+                             "insert_p50_ms": round(1e3 * float(np.percentile(lat_i, 50)), 2),
+                             "insert_p99_ms": round(1e3 * float(np.percentile(lat_i, 99)), 2),
+                             "queries": n, "query_mops_e2e": round(n / el_q / 1e6, 1),
+                             "query_p50_ms": round(1e3 * float(np.percentile(lat_q, 50)), 2),
+                             "query_p99_ms": round(1e3 * float(np.percentile(lat_q, 99)), 2),
+                             "note": "host numpy buffers in, values out: PCIe-bound end to end"}
+    return res
+
+
 def srv_config_of(kind, n):
     if kind == "ht":
         cfg = pg.data_structs.hash_table_64(n, bucket=8)
@@ -387,7 +564,7 @@ def srv_config_of(kind, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["1", "3", "4", "del"], required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "5", "del"], required=True)
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--tables", type=int, default=1024)
@@ -397,11 +574,11 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=40.0)
     ap.add_argument("--requests", type=int, default=4000)
     ap.add_argument("--plain-requests", type=int, default=1000)
-    ap.add_argument("--rates", type=float, nargs="+", default=[2000.0, 8000.0, 32000.0])
+    ap.add_argument("--rates", type=float, nargs="+", default=[2000.0, 8000.0, 32000.0, 128000.0])
     a = ap.parse_args()
     import torch
     torch.cuda.init()
-    fn = {"1": config1, "3": config3, "4": config4, "del": config_del}[a.config]
+    fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del}[a.config]
     print(json.dumps(fn(a)))
 
 

@@ -48,3 +48,37 @@ def fisher_yates_half(n: int, seed: int) -> np.ndarray:
     """Indices of a seeded random half of range(n) (the remove set of the HT workload)."""
     rng = np.random.default_rng(seed)
     return np.sort(rng.permutation(n)[: n // 2])
+
+
+def _s64(x: int) -> int:
+    return x - (1 << 64) if x >= (1 << 63) else x
+
+
+def device_splitmix64(seed: int, n: int, start: int = 0, device="cuda"):
+    """splitmix64(seed, n, start) computed by torch on `device` (int64 tensor with
+    the same bits as the numpy stream), for workloads too large to build on the host."""
+    import torch
+
+    def lsr(x, s):
+        return torch.bitwise_right_shift(x, s) & ((1 << (64 - s)) - 1)
+
+    z = torch.arange(start + 1, start + n + 1, dtype=torch.int64, device=device)
+    z = z * _s64(int(GAMMA)) + _s64(seed % (1 << 64))
+    z = (z ^ lsr(z, 30)) * _s64(int(M1))
+    z = (z ^ lsr(z, 27)) * _s64(int(M2))
+    z = z ^ lsr(z, 31)
+    # the table sentinels 0 and ~0 become 1 and ~0 - 1 (a 2^-63 event per key)
+    z = torch.where(z == 0, torch.ones_like(z), z)
+    return torch.where(z == -1, torch.full_like(z, -2), z)
+
+
+def device_zipf_ranks(n_items: int, count: int, a: float, seed: int, device="cuda"):
+    """`count` ranks in [0, n_items) drawn from a bounded power law with exponent a
+    (Zipf(a), by inverting the continuous CDF), on `device` (int64)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    u = torch.rand(count, dtype=torch.float64, device=device, generator=g)
+    e = 1.0 - a
+    x = (1.0 + u * ((n_items + 1.0) ** e - 1.0)) ** (1.0 / e)
+    return (x.floor().to(torch.int64) - 1).clamp_(0, n_items - 1)
