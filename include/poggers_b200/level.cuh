@@ -66,7 +66,8 @@ struct level_desc {
     fastmod64 nbmod;       // d = number of buckets
     uint64_t seed, seed2;  // hasher seeds (s, s*s)
     uint32_t bucket_size, max_probes, scheme, probe;
-    uint32_t bucket_bytes, pad;
+    uint32_t bucket_bytes;
+    uint32_t fp_resident;  // 1 when the fingerprint array fits in L2 and is kept there (evict-last loads)
     unsigned char *fp;     // FMT_KV64_FP: one fingerprint byte per slot, else null
 };
 
@@ -765,6 +766,18 @@ __device__ __forceinline__ uint64_t l2_policy_evict_last()
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
+__device__ __forceinline__ uint64_t l2_policy_evict_normal()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// fingerprint loads: kept in L2 (evict-last) while the whole array fits there;
+// a larger array would only crowd out the slot lines of the region in use
+__device__ __forceinline__ uint64_t fp_policy(const level_desc &L)
+{
+    return L.fp_resident ? l2_policy_evict_last() : l2_policy_evict_normal();
+}
 __device__ __forceinline__ uint64_t l2_policy_evict_first()
 {
     uint64_t p;
@@ -861,7 +874,7 @@ struct level_ops_fp {
         probe_seq ps;
         ps.begin(L.probe, key, key, L.seed, L.seed2);
         const uint32_t f = fp_of(key, ps.h1);
-        const uint64_t keep = l2_policy_evict_last();
+        const uint64_t keep = fp_policy(L);
         for (uint32_t i = 0; i < L.max_probes; ++i) {
             const uint64_t raw = ps.at(i);
             if (raw == kProbeEnd) break;
@@ -889,7 +902,7 @@ struct level_ops_fp {
         probe_seq ps;
         ps.begin(L.probe, key, key, L.seed, L.seed2);
         const uint32_t f = fp_of(key, ps.h1);
-        const uint64_t keep = l2_policy_evict_last(), stream = l2_policy_evict_first();
+        const uint64_t keep = fp_policy(L), stream = l2_policy_evict_first();
         for (uint32_t i = 0; i < L.max_probes; ++i) {
             const uint64_t raw = ps.at(i);
             if (raw == kProbeEnd) break;
@@ -921,7 +934,7 @@ struct level_ops_fp {
         probe_seq ps;
         ps.begin(L.probe, key, key, L.seed, L.seed2);
         const uint32_t f = fp_of(key, ps.h1);
-        const uint64_t keep = l2_policy_evict_last();
+        const uint64_t keep = fp_policy(L);
         for (uint32_t i = 0; i < L.max_probes; ++i) {
             const uint64_t raw = ps.at(i);
             if (raw == kProbeEnd) break;

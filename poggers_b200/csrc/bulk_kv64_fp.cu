@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) k_query_fp_refill(table_desc t, bulk_args
     const uint64_t per = (a.n + nwarps - 1) / nwarps;
     uint64_t cursor = warp * per;
     const uint64_t end = cursor + per < a.n ? cursor + per : a.n;
-    const uint64_t keep = l2_policy_evict_last(), stream = l2_policy_evict_first();
+    const uint64_t keep = fp_policy(L), stream = l2_policy_evict_first();
     unsigned long long *vout = static_cast<unsigned long long *>(a.vals_out);
     const uint32_t lt = (1u << lane) - 1u;
     bool active = false;

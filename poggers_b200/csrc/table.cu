@@ -15,6 +15,10 @@ using namespace pg;
 
 namespace {
 
+// largest fingerprint array kept in L2 with evict-last loads (L2 is 126 MB; the
+// slot lines of the buckets in use need the rest)
+constexpr uint64_t kFpResidentBytes = 80ull << 20;
+
 bool packed(uint32_t fmt) { return fmt == PG_FMT_PACKED_TAGVAL16 || fmt == PG_FMT_PACKED_TAGVAL8; }
 uint32_t key_bytes(uint32_t fmt)
 {
@@ -297,6 +301,7 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
                 return cuda_status(e);
             }
             D.fp = static_cast<unsigned char *>(t->fp);
+            D.fp_resident = t->fp_bytes <= kFpResidentBytes;
         }
         s = s * s;  // recursive table gets seed*seed (base_table.cuh:124)
     }
