@@ -71,43 +71,54 @@ struct packed_level {
     static constexpr int N = B / G;  // words per lane
     static_assert(N <= 32, "slots per lane");
 
+    // What an operation needs of one read of a bucket, as lane-local bit masks
+    // over the lane's N words (bit i = word gl*N + i), so the words themselves
+    // die right after the read: empty words, tombstone words, dead tags (empty
+    // or deleted: not counted in the fill), words holding the key's tag, and
+    // the first such word (a remove's expected value).
     struct snap {
-        word w[N];
+        uint32_t empty, tomb, dead, match;
+        word mword;
     };
 
     __device__ __forceinline__ static word *slot(const level_desc &L, uint64_t b, int s)
     {
         return reinterpret_cast<word *>(L.base + b * (uint64_t)L.bucket_bytes) + s;
     }
-    __device__ __forceinline__ static void load(const level_desc &L, const group<G> &g, uint64_t b, snap &s)
+    __device__ __forceinline__ static void load(const level_desc &L, const group<G> &g, uint64_t b, uint32_t t,
+                                                snap &s)
     {
-        load_keys<word, N>(slot(L, b, (int)g.gl * N), s.w);
-    }
-    // lane-local masks over the lane's N words
-    __device__ __forceinline__ static uint32_t m_word(const snap &s, word x)
-    {
-        uint32_t m = 0;
+        word w[N];
+        load_keys<word, N>(slot(L, b, (int)g.gl * N), w);
+        s.empty = s.tomb = s.dead = s.match = 0;
+        s.mword = 0;
 #pragma unroll
-        for (int i = 0; i < N; ++i) m |= (uint32_t)(s.w[i] == x) << i;
-        return m;
-    }
-    __device__ __forceinline__ static uint32_t m_tag(const snap &s, uint32_t t)
-    {
-        uint32_t m = 0;
-#pragma unroll
-        for (int i = 0; i < N; ++i) m |= (uint32_t)(P::tag_of(s.w[i]) == t) << i;
-        return m;
+        for (int i = N - 1; i >= 0; --i) {
+            const uint32_t tg = P::tag_of(w[i]);
+            s.empty |= (uint32_t)(w[i] == (word)0) << i;
+            s.tomb |= (uint32_t)(w[i] == P::kTombWord) << i;
+            s.dead |= (uint32_t)(tg == 0u || tg == P::kMask) << i;
+            if (tg == t) {
+                s.match |= 1u << i;
+                s.mword = w[i];  // descending loop: ends on the lowest match
+            }
+        }
     }
     // live slots of the bucket: neither an empty nor a deleted tag (packed_bucket.cuh:36-60)
     __device__ __forceinline__ static int fill(const group<G> &g, const snap &s)
     {
-        const uint32_t dead = m_tag(s, 0u) | m_tag(s, P::kMask);
-        return (int)g.sum((uint32_t)__popc((~dead) & ((N == 32) ? 0xFFFFFFFFu : ((1u << N) - 1u))));
+        const uint32_t all = (N == 32) ? 0xFFFFFFFFu : ((1u << N) - 1u);
+        return (int)g.sum((uint32_t)__popc((~s.dead) & all));
     }
-    // CAS(snapshot word -> desired) on the marked slots, in slot order; true on the first success
+    // CAS(expected -> desired) on the marked slots, in slot order; true on the
+    // first success.  expected: 0 for an empty word, the tombstone word for a
+    // deleted one, for a match the word read (the first) or read again (later
+    // candidates, after a CAS lost a race; skipped if the tag changed meanwhile).
     __device__ __forceinline__ static bool cas_first(const level_desc &L, const group<G> &g, uint64_t b,
-                                                     const snap &s, uint32_t m, word desired)
+                                                     const snap &s, uint32_t m, word desired, bool by_tag,
+                                                     uint32_t t)
     {
+        const int first_match = s.match ? __ffs(s.match) - 1 : -1;
         while (true) {
             const uint32_t bal = g.ballot(m != 0);
             if (!bal) return false;
@@ -115,21 +126,29 @@ struct packed_level {
             bool ok = false;
             if (g.gl == leader) {
                 const int i = __ffs(m) - 1;
-                const word expect = pick(s.w, i);
-                if (atomicCAS(slot(L, b, (int)g.gl * N + i), expect, desired) == expect) ok = true;
+                word *p = slot(L, b, (int)g.gl * N + i);
+                bool go = true;
+                word expect;
+                if (!by_tag) {
+                    expect = ((s.empty >> i) & 1u) ? (word)0 : P::kTombWord;
+                } else if (i == first_match) {
+                    expect = s.mword;
+                } else {
+                    expect = ldcg_scalar(p);
+                    go = P::tag_of(expect) == t;
+                }
+                if (go && atomicCAS(p, expect, desired) == expect) ok = true;
                 else m &= m - 1;
             }
             if (g.ballot(ok)) return true;
         }
     }
-    // first slot holding tag t: its value (packed_bucket.cuh:182-212)
-    __device__ __forceinline__ static bool query_in(const group<G> &g, const snap &s, uint32_t t, V &out)
+    // first slot holding the tag: its value (packed_bucket.cuh:182-212)
+    __device__ __forceinline__ static bool query_in(const group<G> &g, const snap &s, V &out)
     {
-        const uint32_t m = m_tag(s, t);
-        const uint32_t bal = g.ballot(m != 0);
+        const uint32_t bal = g.ballot(s.match != 0);
         if (!bal) return false;
-        const uint32_t ln = __ffs(bal) - 1;
-        const word w = g.shfl(m ? pick(s.w, __ffs(m) - 1) : (word)0, ln);
+        const word w = g.shfl(s.mword, __ffs(bal) - 1);
         out = P::val_of(w);
         return true;
     }
@@ -137,22 +156,21 @@ struct packed_level {
     __device__ __forceinline__ static bool place_in(const level_desc &L, const group<G> &g, uint64_t b,
                                                     const snap &s, word nw, bool reuse)
     {
-        uint32_t m = m_word(s, (word)0);
-        if (reuse) m |= m_word(s, P::kTombWord);
-        return cas_first(L, g, b, s, m, nw);
+        return cas_first(L, g, b, s, reuse ? (s.empty | s.tomb) : s.empty, nw, false, 0);
     }
     // remove (:220-264): the first slot holding the tag becomes the tombstone word
     __device__ __forceinline__ static bool remove_in(const level_desc &L, const group<G> &g, uint64_t b,
                                                      const snap &s, uint32_t t)
     {
-        return cas_first(L, g, b, s, m_tag(s, t), P::kTombWord);
+        return cas_first(L, g, b, s, s.match, P::kTombWord, true, t);
     }
 
     // ---------------------------------------------------------------- schemes
     // two-choice shortcut placement (power_of_n_shortcut_buckets.cuh:198-419):
     // a probed bucket with fill below 3/4 of B takes the key at once; if none
     // does, buckets are retried in increasing fill order, ties in probe order.
-    __device__ static bool tc_place(const level_desc &L, const group<G> &g, probe_seq &ps, word nw, bool reuse)
+    __device__ static bool tc_place(const level_desc &L, const group<G> &g, probe_seq &ps, uint32_t t, word nw,
+                                    bool reuse)
     {
         uint64_t bk[kTwoChoiceMaxProbes];
         int fl[kTwoChoiceMaxProbes];
@@ -170,7 +188,7 @@ struct packed_level {
             }
             bk[j] = L.nbmod.mod(raw);
             snap s;
-            load(L, g, bk[j], s);
+            load(L, g, bk[j], t, s);
             int f = fill(g, s);
             if (4 * f < 3 * B) {
                 if (place_in(L, g, bk[j], s, nw, reuse)) return true;
@@ -186,7 +204,7 @@ struct packed_level {
             for (int j = 0; j < kTwoChoiceMaxProbes; ++j) {
                 if (fl[j] == i) {
                     snap s;
-                    load(L, g, bk[j], s);
+                    load(L, g, bk[j], t, s);
                     if (place_in(L, g, bk[j], s, nw, reuse)) return true;
                 }
                 if (fl[j] > i && fl[j] < next) next = fl[j];
@@ -198,7 +216,8 @@ struct packed_level {
 
     // One operation on this level.  Returns the reference scheme's boolean;
     // out / found are its ext_val / found_val.
-    __device__ static bool op(const level_desc &L, const group<G> &g, int opk, uint64_t key, uint64_t val, V &out,
+    __device__ __forceinline__ static bool op(const level_desc &L, const group<G> &g, int opk, uint64_t key,
+                                              uint64_t val, V &out,
                               bool &found)
     {
         const uint64_t t = P::tag(key);
@@ -210,14 +229,14 @@ struct packed_level {
         case POP_INSERT:
         case POP_INSERT_DELETE: {
             const bool reuse = opk == POP_INSERT_DELETE;
-            if (!linear) return tc_place(L, g, ps, nw, reuse);
+            if (!linear) return tc_place(L, g, ps, (uint32_t)t, nw, reuse);
             // linear_insert_buckets.cuh:192-236: the first probed bucket that takes it
             for (uint32_t i = 0; i < L.max_probes; ++i) {
                 const uint64_t raw = ps.at(i);
                 if (raw == kProbeEnd) break;
                 const uint64_t b = L.nbmod.mod(raw);
                 snap s;
-                load(L, g, b, s);
+                load(L, g, b, (uint32_t)t, s);
                 if (place_in(L, g, b, s, nw, reuse)) return true;
             }
             return false;
@@ -231,9 +250,9 @@ struct packed_level {
                 if (raw == kProbeEnd) break;
                 const uint64_t b = L.nbmod.mod(raw);
                 snap s;
-                load(L, g, b, s);
+                load(L, g, b, (uint32_t)t, s);
                 if (opk == POP_QUERY) {
-                    if (query_in(g, s, (uint32_t)t, out)) return true;
+                    if (query_in(g, s, out)) return true;
                 } else {
                     if (remove_in(L, g, b, s, (uint32_t)t)) return true;
                 }
@@ -253,14 +272,14 @@ struct packed_level {
                     if (raw == kProbeEnd) break;
                     const uint64_t b = L.nbmod.mod(raw);
                     snap s;
-                    load(L, g, b, s);
-                    if (query_in(g, s, (uint32_t)t, out)) {
+                    load(L, g, b, (uint32_t)t, s);
+                    if (query_in(g, s, out)) {
                         found = true;
                         if (del) remove_in(L, g, b, s, (uint32_t)t);
                         return true;
                     }
                 }
-                return tc_place(L, g, ps, nw, del);
+                return tc_place(L, g, ps, (uint32_t)t, nw, del);
             }
             // linear_insert_buckets.cuh:238-330: per probe, query, then a plain insert
             for (uint32_t i = 0; i < L.max_probes; ++i) {
@@ -268,8 +287,8 @@ struct packed_level {
                 if (raw == kProbeEnd) break;
                 const uint64_t b = L.nbmod.mod(raw);
                 snap s;
-                load(L, g, b, s);
-                if (query_in(g, s, (uint32_t)t, out)) {
+                load(L, g, b, (uint32_t)t, s);
+                if (query_in(g, s, out)) {
                     found = true;
                     if (del) remove_in(L, g, b, s, (uint32_t)t);
                     return true;
