@@ -353,3 +353,26 @@ def test_fingerprints_with_backing_level_matches_oracle(pg, oracle):
     fo, vo = o.query_many(q)
     assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
     assert (f[:n] == ok).all()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_slot_cas_succeeds_once_under_contention(pg, layout):
+    """key_val_pair::atomic_swap succeeds once per empty slot
+    (tests/src/test_key_val_pair.cu:50-122): 256 keys raced into a one-bucket
+    table (8 slots, one probe) from 256 groups at once place exactly 8 keys,
+    each exactly once, and every placed key answers with its own value."""
+    cfg = pg.TableConfig(pg.FMT_KV64, 4, [pg.Level(8, 8, 1, 0, 1)])
+    cfg.split = layout == "split"
+    cfg.fingerprints = layout == "fingerprints"
+    t = pg.Table(cfg, 3)
+    d = Driver(t)
+    keys = wl.keys_without_sentinels(61, 256)
+    vals = wl.values_for(keys, 8, 62)
+    ok = d.insert(keys, vals)
+    assert ok.sum() == 8
+    assert t.get_fill(0) == (8, 0)
+    f, v = d.query(keys)
+    assert (f == ok).all() and (v[ok] == vals[ok]).all()
+    # a second insert of a placed key finds no empty slot (the bucket is full)
+    ok2 = d.insert(keys[ok][:1], vals[ok][:1])
+    assert not ok2.any()
