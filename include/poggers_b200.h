@@ -264,7 +264,9 @@ pg_status pg_table_load_image(const void *host_src, uint64_t bytes, pg_table **o
  * conflict on one table (an insert or remove with anything else on that
  * table) belong in separate runs (stream-ordered).
  * --------------------------------------------------------------------------- */
-enum { PG_OP_INSERT = 0, PG_OP_QUERY = 1, PG_OP_REMOVE = 2 };
+/* PG_OP_INSERT_WITH_DELETE: bucketed_table::insert_with_delete, for tables of
+ * the packed formats only (requests of it on other tables are skipped). */
+enum { PG_OP_INSERT = 0, PG_OP_QUERY = 1, PG_OP_REMOVE = 2, PG_OP_INSERT_WITH_DELETE = 3 };
 
 typedef struct pg_op_desc {
     uint32_t table;  /* index into the batch's table list */

@@ -93,7 +93,7 @@ EXPORTED = (
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
 )
-PG_OP_INSERT, PG_OP_QUERY, PG_OP_REMOVE = 0, 1, 2
+PG_OP_INSERT, PG_OP_QUERY, PG_OP_REMOVE, PG_OP_INSERT_WITH_DELETE = 0, 1, 2, 3
 
 
 def lib() -> C.CDLL:

@@ -16,6 +16,7 @@ struct pg_batch {
     uint32_t ntables;
     uint32_t max_ops;
     uint32_t ifmt, bucket, scheme;
+    uint32_t bucket1;  // backing level's bucket size (the bucketed filter's kernels take it as a parameter)
     bool backing;
     table_desc *d_tables;
     unsigned long long *d_scratch;  // chunk_start[max_ops + 1] then the work counter
@@ -113,6 +114,23 @@ pg_status static_scratch_addr(static_scratch **out)
 
 }  // namespace
 
+namespace {
+
+bool packed_fmt(uint32_t ifmt) { return ifmt == FMT_PACKED16 || ifmt == FMT_PACKED8; }
+
+uint32_t backing_bucket(const pg_table *t) { return t->cfg.nlevels > 1 ? t->cfg.levels[1].bucket_size : 0; }
+
+// one kernel instantiation serves a batch: same format, bucket, scheme and depth
+// (and, for the bucketed filter, the same backing bucket size)
+bool same_kernel(const pg_table *t, const pg_table *t0)
+{
+    return t && t->ifmt == t0->ifmt && t->cfg.levels[0].bucket_size == t0->cfg.levels[0].bucket_size &&
+           t->cfg.levels[0].scheme == t0->cfg.levels[0].scheme && (t->cfg.nlevels > 1) == (t0->cfg.nlevels > 1) &&
+           (!packed_fmt(t0->ifmt) || backing_bucket(t) == backing_bucket(t0)) && t->device == t0->device;
+}
+
+}  // namespace
+
 extern "C" {
 
 pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t max_ops, pg_batch **out)
@@ -121,14 +139,10 @@ pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t ma
     *out = nullptr;
     const pg_table *t0 = tables[0];
     if (!t0) return PG_ERR_INVALID;
-    if (t0->ifmt == FMT_PACKED16 || t0->ifmt == FMT_PACKED8) return PG_ERR_UNSUPPORTED;  // bulk calls only
     for (uint32_t i = 1; i < ntables; i++) {
         const pg_table *t = tables[i];
         // one kernel instantiation serves the batch: same format, bucket, scheme and depth
-        if (!t || t->ifmt != t0->ifmt || t->cfg.levels[0].bucket_size != t0->cfg.levels[0].bucket_size ||
-            t->cfg.levels[0].scheme != t0->cfg.levels[0].scheme || (t->cfg.nlevels > 1) != (t0->cfg.nlevels > 1) ||
-            t->device != t0->device)
-            return PG_ERR_UNSUPPORTED;
+        if (!same_kernel(t, t0)) return PG_ERR_UNSUPPORTED;
     }
     pg_batch *b = (pg_batch *)calloc(1, sizeof(pg_batch));
     if (!b) return PG_ERR_NOMEM;
@@ -138,6 +152,7 @@ pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t ma
     b->bucket = t0->cfg.levels[0].bucket_size;
     b->scheme = t0->cfg.levels[0].scheme;
     b->backing = t0->cfg.nlevels > 1;
+    b->bucket1 = backing_bucket(t0);
     b->num_sms = t0->num_sms;
     b->block_threads = 256;
     b->blocks_per_sm = 8;
@@ -173,6 +188,7 @@ pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t bloc
     if (blocks_per_sm == 0) blocks_per_sm = 8;
     if (lanes_per_key == 0) lanes_per_key = b->lanes;
     if (b->ifmt == FMT_KV64_FP) lanes_per_key = 1;
+    if (packed_fmt(b->ifmt)) lanes_per_key = lanes_per_key >= 4 ? 4 : 1;  // the widths built for the bucketed filter
     if (!(lanes_per_key == 1 || lanes_per_key == 2 || lanes_per_key == 4 || lanes_per_key == 8 ||
           lanes_per_key == 16) ||
         lanes_per_key > b->bucket)
@@ -214,6 +230,8 @@ pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_n
     case FMT_TAGVAL16: e = batch_tagval16(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
     case FMT_TAGVAL16_SPLIT: e = batch_tagval16_split(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
     case FMT_KV64_FP: e = batch_kv64_fp(a, b->bucket, 1, sch, b->backing, grid, block, s); break;
+    case FMT_PACKED16:
+    case FMT_PACKED8: e = batch_packed(a, b->ifmt, b->bucket, b->bucket1, b->lanes, b->backing, grid, block, s); break;
     default: e = batch_tag16(a, b->bucket, b->lanes, sch, b->backing, grid, block, s); break;
     }
     if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;
@@ -229,13 +247,9 @@ pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const p
     if (ntables > kStaticMaxTables || max_ops > kStaticMaxOps) return PG_ERR_TOO_LARGE;
     const pg_table *t0 = tables[0];
     if (!t0) return PG_ERR_INVALID;
-    if (t0->ifmt == FMT_PACKED16 || t0->ifmt == FMT_PACKED8) return PG_ERR_UNSUPPORTED;  // bulk calls only
     for (uint32_t i = 1; i < ntables; i++) {
         const pg_table *t = tables[i];
-        if (!t || t->ifmt != t0->ifmt || t->cfg.levels[0].bucket_size != t0->cfg.levels[0].bucket_size ||
-            t->cfg.levels[0].scheme != t0->cfg.levels[0].scheme || (t->cfg.nlevels > 1) != (t0->cfg.nlevels > 1) ||
-            t->device != t0->device)
-            return PG_ERR_UNSUPPORTED;
+        if (!same_kernel(t, t0)) return PG_ERR_UNSUPPORTED;
     }
     std::lock_guard<std::mutex> g(g_static_mu);
     static_scratch *sc = nullptr;
@@ -274,6 +288,8 @@ pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const p
     case FMT_TAGVAL16: e = batch_tagval16(a, bucket, lanes, sch, bk, grid, block, s); break;
     case FMT_TAGVAL16_SPLIT: e = batch_tagval16_split(a, bucket, lanes, sch, bk, grid, block, s); break;
     case FMT_KV64_FP: e = batch_kv64_fp(a, bucket, 1, sch, bk, grid, block, s); break;
+    case FMT_PACKED16:
+    case FMT_PACKED8: e = batch_packed(a, t0->ifmt, bucket, backing_bucket(t0), lanes, bk, grid, block, s); break;
     default: e = batch_tag16(a, bucket, lanes, sch, bk, grid, block, s); break;
     }
     if (e == cudaErrorInvalidConfiguration) return PG_ERR_UNSUPPORTED;

@@ -153,5 +153,8 @@ PG_DECLARE_BATCH(batch_tagval16);
 PG_DECLARE_BATCH(batch_tagval16_split);
 PG_DECLARE_BATCH(batch_tag16);
 PG_DECLARE_BATCH(batch_kv64_fp);
+// the bucketed filter: level-0 bucket b0, backing bucket b1 (packed formats)
+cudaError_t batch_packed(const batch_args &a, uint32_t ifmt, uint32_t b0, uint32_t b1, uint32_t lanes, bool bk,
+                         dim3 grid, dim3 block, cudaStream_t s);
 
 }  // namespace pg

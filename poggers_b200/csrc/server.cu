@@ -110,7 +110,9 @@ namespace {
 
 uint32_t class_key(const pg_table *t)
 {
-    return (t->ifmt << 24) | (t->cfg.levels[0].bucket_size << 8) | (t->cfg.levels[0].scheme << 4) |
+    const bool packed = t->ifmt == pg::FMT_PACKED16 || t->ifmt == pg::FMT_PACKED8;
+    const uint32_t b1 = packed && t->cfg.nlevels > 1 ? t->cfg.levels[1].bucket_size : 0u;
+    return (t->ifmt << 24) | (b1 << 16) | (t->cfg.levels[0].bucket_size << 8) | (t->cfg.levels[0].scheme << 4) |
            (t->cfg.nlevels > 1 ? 1u : 0u);
 }
 
@@ -251,7 +253,7 @@ void worker_loop(pg_server *s)
                 const uint32_t vb = s->classes[te.cls].vbytes;
                 slots[w].key_off[i] = ko;
                 memcpy(st.h_keys + ko, r->keys, r->n * 8);
-                if (r->op == PG_OP_INSERT && vb) {
+                if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
                     unsigned char *dst = (vb == 8 ? st.h_vin : st.h_vin16) + ko * vb;
                     if (r->vals) memcpy(dst, r->vals, r->n * vb);
                     else memset(dst, 0, r->n * vb);
@@ -400,10 +402,14 @@ pg_status pg_server_destroy(pg_server *s)
 pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t seed, uint32_t *table_id)
 {
     if (!s || !cfg || !table_id) return PG_ERR_INVALID;
-    if (cfg->format == PG_FMT_PACKED_TAGVAL16 || cfg->format == PG_FMT_PACKED_TAGVAL8) return PG_ERR_UNSUPPORTED;
+    // staging holds 64- and 16-bit values: the 8-bit bucketed filter is served by the bulk calls only
+    if (cfg->format == PG_FMT_PACKED_TAGVAL8) return PG_ERR_UNSUPPORTED;
     // admission by HBM budget: the table's slot arrays (and fingerprints) must fit
     uint64_t need = 0;
-    const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : 2, vb = cfg->format == PG_FMT_KV64 ? 8 : (cfg->format == PG_FMT_TAGVAL16 ? 2 : 0);
+    const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : 2;
+    const uint32_t vb = cfg->format == PG_FMT_KV64 ? 8
+                        : (cfg->format == PG_FMT_TAGVAL16 || cfg->format == PG_FMT_PACKED_TAGVAL16) ? 2
+                                                                                                    : 0;
     for (uint32_t l = 0; l < cfg->nlevels && l < 2; l++) {
         const pg_level_config &L = cfg->levels[l];
         if (L.bucket_size == 0 || L.nslots == 0) return PG_ERR_INVALID;
@@ -479,10 +485,11 @@ uint64_t pg_server_bytes_in_use(pg_server *s)
 pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const uint64_t *h_keys, const void *h_vals,
                            uint64_t n, void *h_vals_out, uint8_t *h_flags, uint64_t *request_id)
 {
-    if (!s || !request_id || (n && !h_keys) || op > PG_OP_REMOVE) return PG_ERR_INVALID;
+    if (!s || !request_id || (n && !h_keys) || op > PG_OP_INSERT_WITH_DELETE) return PG_ERR_INVALID;
     if (n > s->cfg.max_wave_keys) return PG_ERR_INVALID;
     std::lock_guard<std::mutex> g(s->mu);
     if (table_id >= s->tables.size() || !s->tables[table_id].live) return PG_ERR_INVALID;
+    if (op == PG_OP_INSERT_WITH_DELETE && s->tables[table_id].t->ifmt != pg::FMT_PACKED16) return PG_ERR_UNSUPPORTED;
     if (s->error != PG_OK) return s->error;
     request *r = new request();
     r->id = s->next_id++;

@@ -188,6 +188,7 @@ def test_packed_formats_reject_unsupported_calls(pg):
     k = to_dev(wl.keys_without_sentinels(1, 10))
     with pytest.raises(pg.PoggersError):
         t.bulk_insert_with_delete(k)
+    # one batch serves tables of one kernel shape: a filter and a hash table do not mix
     with pytest.raises(pg.PoggersError):
-        pg.Batch([pg.Table(pg.data_structs.del_tcf(1 << 12, 64), 1)], 16)
+        pg.Batch([pg.Table(pg.data_structs.del_tcf(1 << 12, 64), 1), t], 16)
     del torch

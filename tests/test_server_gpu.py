@@ -125,3 +125,35 @@ def test_server_admits_tables_by_hbm_budget(pg):
     r = srv.submit(0, 0, k, wl.values_for(k, 8, 1), None, f)
     assert srv.poll(r, wait=True)[0] == 0 and f.all()
     srv.close()
+
+
+def test_server_serves_bucketed_filters(pg):
+    """A 16-bit bucketed filter behind the serving loop: inserts, queries,
+    removes and insert_with_delete requests, each result as the table's own
+    bulk call would give it; 8-bit filters are refused."""
+    srv = pg.Server(hbm_budget_bytes=1 << 30, max_wave_keys=1 << 16, max_wave_requests=64)
+    try:
+        tid = srv.add_table(pg.data_structs.del_tcf(1 << 16, 1 << 10), 7)
+        assert tid is not None
+        with pytest.raises(pg.PoggersError):
+            srv.add_table(pg.data_structs.del_tcf(1 << 12, 1 << 8, tag_bits=8), 8)
+        keys = wl.keys_without_sentinels(21, 40000)
+        vals = (wl.values_for(keys, 2, 22).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
+        fl = np.zeros(len(keys), dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_INSERT, keys, vals, None, fl), wait=True)
+        assert fl.all()
+        vo = np.zeros(len(keys), dtype=np.uint16)
+        fq = np.zeros(len(keys), dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_QUERY, keys, None, vo, fq), wait=True)
+        assert fq.all() and (vo == vals).mean() > 0.999
+        fr = np.zeros(20000, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_REMOVE, keys[:20000], None, None, fr), wait=True)
+        assert fr.all()
+        fa = np.zeros(20000, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_INSERT_WITH_DELETE, keys[:20000], vals[:20000], None, fa), wait=True)
+        assert fa.all()
+        fq2 = np.zeros(len(keys), dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_QUERY, keys, None, None, fq2), wait=True)
+        assert fq2.all()
+    finally:
+        srv.close()
