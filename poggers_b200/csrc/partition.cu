@@ -21,6 +21,7 @@
 #include "poggers_b200.h"
 #include "bulk_kernels.cuh"
 #include "table_internal.h"
+#include "bulk_packed.cuh"
 
 namespace pg {
 
@@ -193,11 +194,15 @@ using namespace pg;
 // leaves `a` alone) when the batch should take the ordinary path: partitioning
 // off, a serial launch shape, not a uint64 bucket table, table or batch too
 // small for the sort to pay, or no memory for the scratch.
-bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
+namespace {
+
+// The region sort shared by the uint64 tables and the bucketed filter: sorts
+// (keys, values of vbytes) into the table's scratch, presets the flags to 1,
+// and returns the sorted copy and the permutation; false when the batch
+// should run in batch order.
+bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&vals, uint32_t vbytes, uint8_t *flags,
+                 const uint32_t *&perm, cudaStream_t s)
 {
-    const uint64_t n = a.n;
-    const bool kv64 = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT || t->ifmt == FMT_KV64_FP;
-    if (!t->partition || !kv64 || t->cfg.levels[0].scheme != PG_SCHEME_BUCKET || t->max_blocks == 1) return false;
     if (t->bytes[0] < 2 * kPartRegionBytes || n < kPartMinKeys || n >= (1ull << 32)) return false;
     // regions of 2^shift buckets, about kPartRegionBytes of slots each, at most kPartMaxRegions
     const uint64_t nb = t->desc.lv[0].nbmod.d, bucket_bytes = t->bytes[0] / nb;
@@ -205,7 +210,7 @@ bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
     while ((bucket_bytes << (shift + 1)) <= kPartRegionBytes) shift++;
     while (((nb - 1) >> shift) + 1 > kPartMaxRegions) shift++;
     const uint32_t R = (uint32_t)(((nb - 1) >> shift) + 1);
-    // scratch: keys (8 B), values (8 B), original index (4 B) per key; counts and cursors per region
+    // scratch: keys (8 B), values (up to 8 B), original index (4 B) per key; counts and cursors per region
     const uint64_t cnt_off = (n * 20 + 255) & ~255ull;
     const uint64_t need = cnt_off + 2ull * R * 8;
     if (t->part_bytes < need) {
@@ -220,7 +225,7 @@ bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
     }
     unsigned char *p = static_cast<unsigned char *>(t->part_buf);
     uint64_t *okeys = reinterpret_cast<uint64_t *>(p);
-    unsigned long long *ovals = a.vals_in ? reinterpret_cast<unsigned long long *>(p + n * 8) : nullptr;
+    void *ovals = vals ? static_cast<void *>(p + n * 8) : nullptr;
     uint32_t *operm = reinterpret_cast<uint32_t *>(p + n * 16);
     unsigned long long *counts = reinterpret_cast<unsigned long long *>(p + cnt_off);
     unsigned long long *cursors = counts + R;
@@ -228,15 +233,46 @@ bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
     const unsigned grid = (unsigned)(t->num_sms * 8);
     cudaMemsetAsync(counts, 0, R * 8, s);
     const region_router route{L, shift};
-    k_part_count<<<grid, kPartThreads, 0, s>>>(route, a.keys, n, R, counts);
+    k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, R, counts);
     k_part_scan<<<1, 32, 0, s>>>(counts, cursors, R);
-    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
-                                                 R, cursors, okeys, ovals, operm);
-    if (a.flags) cudaMemsetAsync(a.flags, 1, n, s);
-    a.keys = okeys;
-    a.vals_in = ovals;
-    a.perm = operm;
+    switch (vbytes) {
+    case 2:
+        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned short *>(vals), n, R,
+                                                     cursors, okeys, static_cast<unsigned short *>(ovals), operm);
+        break;
+    case 1:
+        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned char *>(vals), n, R,
+                                                     cursors, okeys, static_cast<unsigned char *>(ovals), operm);
+        break;
+    default:
+        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned long long *>(vals), n,
+                                                     R, cursors, okeys, static_cast<unsigned long long *>(ovals),
+                                                     operm);
+        break;
+    }
+    if (flags) cudaMemsetAsync(flags, 1, n, s);
+    keys = okeys;
+    vals = ovals;
+    perm = operm;
     return true;
+}
+
+}  // namespace
+
+bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
+{
+    const bool kv64 = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT || t->ifmt == FMT_KV64_FP;
+    if (!t->partition || !kv64 || t->cfg.levels[0].scheme != PG_SCHEME_BUCKET || t->max_blocks == 1) return false;
+    return region_sort(t, a.n, a.keys, a.vals_in, 8, a.flags, a.perm, s);
+}
+
+// The bucketed filter's inserts: the first probe of both of its schemes is
+// bucket MurmurHash64A(key, seed) % nb, the bucket the regions are cut by.
+bool pg_partition_packed(pg_table *t, packed_args &a, cudaStream_t s)
+{
+    const bool packed = t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8;
+    if (!t->partition || !packed || t->max_blocks == 1) return false;
+    return region_sort(t, a.n, a.keys, a.vals_in, t->ifmt == FMT_PACKED16 ? 2u : 1u, a.flags, a.perm, s);
 }
 
 // ---------------------------------------------------------------- sharding
