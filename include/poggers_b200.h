@@ -393,6 +393,13 @@ pg_status pg_slab_count_free(pg_slab *a, uint64_t *d_out, pg_stream_t stream);
 pg_status pg_slab_report(pg_slab *a, uint64_t *free_slabs, uint64_t *max_slabs, uint64_t *free_objects,
                          uint64_t *double_frees);
 
+/* The device-side descriptor of the pool, for device callers compiled against
+ * include/poggers_b200/slab.cuh (the template API's one_size_slab_allocator
+ * copies it into its device struct): `bytes` must equal sizeof(pg::slab_desc).
+ * Replaces the device struct that one_size_slab_allocator::generate_on_device
+ * builds (allocators/slab_one_size.cuh:84-141). */
+pg_status pg_slab_desc(const pg_slab *a, void *out_desc, uint64_t bytes);
+
 /* Size classes: one pool per class (class_bytes strictly increasing, at most
  * PG_SLAB_MAX_CLASSES).  A request of s bytes is served by the smallest class
  * with class_bytes >= s; larger requests get NULL. */

@@ -87,7 +87,7 @@ EXPORTED = (
     "pg_host_murmur64a", "pg_host_fastmod", "pg_host_probe_buckets",
     "pg_host_shard_of", "pg_route_by_shard", "pg_scatter_by_perm",
     "pg_slab_create", "pg_slab_destroy", "pg_slab_reset", "pg_slab_info", "pg_slab_bulk_malloc",
-    "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_set_create", "pg_slab_set_destroy",
+    "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_desc", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
     "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",

@@ -230,6 +230,13 @@ pg_status pg_slab_bulk_malloc(pg_slab *a, uint64_t n, void **d_ptrs, uint64_t *d
     return cuda_status(cudaGetLastError());
 }
 
+pg_status pg_slab_desc(const pg_slab *a, void *out_desc, uint64_t bytes)
+{
+    if (!a || !out_desc || bytes != sizeof(slab_desc)) return PG_ERR_INVALID;
+    memcpy(out_desc, &a->d, sizeof(slab_desc));
+    return PG_OK;
+}
+
 pg_status pg_slab_bulk_free(pg_slab *a, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count, pg_stream_t stream)
 {
     if (!a || (n && !d_ptrs)) return PG_ERR_INVALID;

@@ -1,0 +1,89 @@
+// test_slab_api.cu -- device callers of the slab allocator written against
+// the reference's template API, compiled against poggers_b200/allocators.cuh.
+//
+// Follows the reference's own drivers (tests/src/slab_one_size_tests.cu:
+// allocate_into_array, the duplicate check of allocate_into_array_bits, and
+// free_from_array): every thread mallocs one object and writes into it, a
+// bitmap over object offsets catches any object handed out twice, every
+// object is freed, the whole pool is allocated a second time, and a second
+// free of the same object is counted.  Prints one JSON line.
+#include <cstdio>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "poggers_b200/allocators.cuh"
+
+namespace pb = poggers_b200;
+using allocator = pb::allocators::one_size_slab_allocator<15>;
+
+__global__ void allocate_into_array_bits(allocator *a, uint64_t *ptrs, uint64_t *bitmap, uint64_t n,
+                                         unsigned long long *c)
+{
+    uint64_t tid = threadIdx.x + (uint64_t)blockIdx.x * blockDim.x;
+    if (tid >= n) return;
+    void *p = a->malloc();
+    ptrs[tid] = (uint64_t)p;
+    if (!p) {
+        atomicAdd(c + 0, 1ULL);  // misses
+        return;
+    }
+    ((char *)p)[0] = 't';
+    uint64_t off = a->get_offset_from_ptr(p);
+    if (off >= a->get_largest_allocation_offset()) atomicAdd(c + 1, 1ULL);  // out of the pool
+    unsigned long long old = atomicOr((unsigned long long *)&bitmap[off / 64], 1ULL << (off % 64));
+    if (old & (1ULL << (off % 64))) atomicAdd(c + 2, 1ULL);  // handed out twice
+}
+
+__global__ void free_from_array(allocator *a, uint64_t *ptrs, uint64_t n)
+{
+    uint64_t tid = threadIdx.x + (uint64_t)blockIdx.x * blockDim.x;
+    if (tid >= n) return;
+    void *p = (void *)ptrs[tid];
+    if (p) a->free(p);
+}
+
+__global__ void double_free(allocator *a, uint64_t *ptrs, uint64_t *misses)
+{
+    if (threadIdx.x + blockIdx.x * blockDim.x != 0) return;
+    void *p = (void *)ptrs[0];
+    a->free_count_misses(p, misses);
+    a->free_count_misses(p, misses);  // the second one is refused
+}
+
+int main()
+{
+    const uint64_t n = 1ULL << 20;  // 256 slabs of 4096, exactly full
+    allocator *a = allocator::generate_on_device(n, 16);
+    uint64_t *ptrs, *bitmap;
+    unsigned long long *c;
+    cudaMalloc(&ptrs, n * 8);
+    cudaMalloc(&bitmap, n / 8);
+    cudaMalloc(&c, 8 * 8);
+    cudaMemset(c, 0, 8 * 8);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    cudaMemset(bitmap, 0, n / 8);
+    allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c);
+    cudaDeviceSynchronize();
+    const uint64_t fill_full = a->report_fill(), slabs = a->report_max();
+    free_from_array<<<blocks, 256>>>(a, ptrs, n);
+    cudaDeviceSynchronize();
+    const uint64_t fill_empty = a->report_fill();
+    cudaMemset(bitmap, 0, n / 8);
+    allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c + 3);
+    cudaDeviceSynchronize();
+    double_free<<<1, 32>>>(a, ptrs, (uint64_t *)(c + 6));
+    cudaError_t e = cudaDeviceSynchronize();
+    unsigned long long h[8];
+    cudaMemcpy(h, c, sizeof(h), cudaMemcpyDeviceToHost);
+    allocator::free_on_device(a);
+    cudaFree(ptrs);
+    cudaFree(bitmap);
+    cudaFree(c);
+    printf("{\"allocs\": %llu, \"misses\": %llu, \"out_of_pool\": %llu, \"duplicates\": %llu, "
+           "\"misses_2\": %llu, \"out_of_pool_2\": %llu, \"duplicates_2\": %llu, \"double_free_refused\": %llu, "
+           "\"free_slabs_when_full\": %llu, \"free_slabs_after_free\": %llu, \"slabs\": %llu, \"cuda\": %d}\n",
+           (unsigned long long)n, h[0], h[1], h[2], h[3], h[4], h[5], h[6], (unsigned long long)fill_full,
+           (unsigned long long)fill_empty, (unsigned long long)slabs, (int)e);
+    const bool ok = e == cudaSuccess && !h[0] && !h[1] && !h[2] && !h[3] && !h[4] && !h[5] && h[6] == 1 &&
+                    fill_full == 0 && fill_empty == slabs;
+    return ok ? 0 : 1;
+}

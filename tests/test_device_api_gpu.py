@@ -7,7 +7,10 @@ test_components.cu (keys id*39, values key*44, insert then query on the same
 tile) and the TCF alias driven by device kernels, then by the bulk C ABI.
 test_bucketed_api: the reference's delete-test kernels on its del_TCF and
 del_TCF_small instantiations (bucketed_table with insert_with_delete and
-insert_if_not_exists)."""
+insert_if_not_exists).
+test_slab_api: the reference's slab allocator drivers on
+one_size_slab_allocator (malloc / free from device code, duplicate check,
+report_fill / report_max, a refused double free)."""
 import json
 import subprocess
 
@@ -47,3 +50,12 @@ def test_bucketed_table_device_api(drivers):
         assert c["fill_final"] == c["fill_after_delete"] + half - c["readd_fail"]
         # every key is present after the re-add, so insert_if_not_exists finds it
         assert c["ine_fail"] == 0 and c["ine_not_found"] <= 20, (name, c)
+
+
+def test_slab_allocator_device_api(drivers):
+    r = subprocess.run([str(drivers["test_slab_api"])], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["misses"] == 0 and d["duplicates"] == 0 and d["out_of_pool"] == 0
+    assert d["misses_2"] == 0 and d["duplicates_2"] == 0 and d["double_free_refused"] == 1
+    assert d["free_slabs_when_full"] == 0 and d["free_slabs_after_free"] == d["slabs"] == d["allocs"] // 4096
