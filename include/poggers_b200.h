@@ -190,7 +190,10 @@ pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t
  * kept by the table (counted in pg_table_bytes) until pg_table_destroy.
  * Concurrent inserts have no defined order in the reference either: which
  * keys fail when a table overflows may differ, every placed key is
- * placed by the same rule. */
+ * placed by the same rule.  The scratch is the table's: two region-ordered
+ * inserts into one table must be ordered on one stream, and the first one
+ * (or one larger than any before) allocates, so make it before any stream
+ * capture or turn region ordering off. */
 pg_status pg_table_set_partitioned_insert(pg_table *t, int enable);
 
 /* Bulk insert of n keys (and values; d_vals may be NULL = all 0).
