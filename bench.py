@@ -317,8 +317,25 @@ def run_e2e(args, table, keys, vals, qkeys, dev, world):
     el = allreduce_max(el * 1e3, world) / 1e3
     assert (h_found[: n // 2].numpy().astype(bool) == h_ok[: n // 2].numpy().astype(bool)).all()
     value = (n + nq) * steps * world / el / 1e6
+    # the link itself: one large pinned copy each way, timed on the device
+    probe = 1 << 30
+    hb = torch.empty(probe, dtype=torch.uint8).pin_memory()
+    db = torch.empty(probe, dtype=torch.uint8, device=dev)
+    link = {}
+    for name, dst, src in (("h2d", db, hb), ("d2h", hb, db)):
+        for _ in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+        link[name] = probe / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del hb, db
+    h2d_rate = (16 * n + 8 * nq) * steps / el / 1e9
     return {"value": round(value, 1), "unit": "Mops/s", "h2d_bytes_per_step": 16 * n + 8 * nq,
             "d2h_bytes_per_step": n + 9 * nq, "steps": steps,
+            "link_h2d_gbs": round(link["h2d"], 1), "link_d2h_gbs": round(link["d2h"], 1),
+            "h2d_gbs_achieved": round(h2d_rate, 1), "h2d_frac_of_link": round(h2d_rate / link["h2d"], 3),
             "note": "host-timed around cudaMemcpyAsync H2D (pinned) + kernels + D2H, 8 chunks per phase, "
                     "uploads and downloads on separate streams"}
 
