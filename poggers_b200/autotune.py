@@ -99,7 +99,9 @@ def best(results: list[Result]) -> Result:
 
 def cache_key(gpu_name: str, config) -> str:
     L = config.levels[0]
-    return f"{gpu_name}|fmt{config.format}|b{L.bucket_size}|s{L.scheme}|p{L.probe}|n{L.nslots.bit_length()}|lv{len(config.levels)}"
+    fp = int(bool(getattr(config, "fingerprints", False)))
+    return (f"{gpu_name}|fmt{config.format}|b{L.bucket_size}|s{L.scheme}|p{L.probe}|n{L.nslots.bit_length()}"
+            f"|lv{len(config.levels)}|fp{fp}")
 
 
 def tuned_shape(config, seed: int, keys, vals, qkeys, **grid) -> Shape:
@@ -115,7 +117,8 @@ def tuned_shape(config, seed: int, keys, vals, qkeys, **grid) -> Shape:
         import poggers_b200 as pg
         lv = [pg.Level(l.nslots, l.bucket_size if (i or bucket is None) else bucket, l.max_probes, l.scheme, l.probe)
               for i, l in enumerate(config.levels)]
-        return pg.TableConfig(config.format, tile, lv)
+        return pg.TableConfig(config.format, tile, lv, getattr(config, "split", False),
+                              getattr(config, "fingerprints", False))
 
     res = sweep(make, seed, keys, vals, qkeys, **grid)
     b = best(res)
