@@ -91,9 +91,9 @@ struct pg_server {
     // staging (per wave slot): pinned host and device buffers
     struct stage {
         uint64_t *h_keys, *d_keys;
-        // values by width (uint64 and uint16 tables), indexed like the keys
-        unsigned char *h_vin, *d_vin, *h_vout, *d_vout;
-        unsigned char *h_vin16, *d_vin16, *h_vout16, *d_vout16;
+        // values by width (8, 2 and 1 bytes: uint64 tables, 16- and 8-bit
+        // filters), each indexed like the keys; see width_index
+        unsigned char *h_vin[3], *d_vin[3], *h_vout[3], *d_vout[3];
         uint8_t *h_flags, *d_flags;
         pg_op_desc *h_ops, *d_ops;
         uint32_t *h_nops, *d_nops;
@@ -117,6 +117,10 @@ uint32_t class_key(const pg_table *t)
 }
 
 bool conflicts(uint32_t a, uint32_t b) { return a != b; }
+
+// staging buffer of a value width: 8 -> 0, 2 -> 1, 1 -> 2
+int width_index(uint32_t vb) { return vb == 8 ? 0 : vb == 2 ? 1 : 2; }
+constexpr uint32_t kWidths[3] = {8, 2, 1};
 
 pg_status rebuild(pg_server *s, klass &k)
 {
@@ -179,7 +183,7 @@ void complete_stage(pg_server *s, pg_server::stage &st, std::vector<request *> &
         const uint32_t vb = s->classes[te.cls].vbytes;
         if (r->flags) memcpy(r->flags, st.h_flags + o, r->n);
         if (r->op == PG_OP_QUERY && r->vals_out && vb)
-            memcpy(r->vals_out, (vb == 8 ? st.h_vout : st.h_vout16) + o * vb, r->n * vb);
+            memcpy(r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb);
         r->count = st.h_counts[i];
         r->t_done = now_s();
         i++;
@@ -246,7 +250,7 @@ void worker_loop(pg_server *s)
             });
             slots[w].key_off.assign(reqs.size(), 0);
             uint64_t ko = 0;
-            bool any_in64 = false, any_in16 = false, any_q64 = false, any_q16 = false;
+            bool any_in[3] = {false, false, false}, any_q[3] = {false, false, false};
             for (size_t i = 0; i < reqs.size(); i++) {
                 request *r = reqs[i];
                 const table_entry &te = s->tables[r->table];
@@ -254,20 +258,21 @@ void worker_loop(pg_server *s)
                 slots[w].key_off[i] = ko;
                 memcpy(st.h_keys + ko, r->keys, r->n * 8);
                 if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
-                    unsigned char *dst = (vb == 8 ? st.h_vin : st.h_vin16) + ko * vb;
+                    unsigned char *dst = st.h_vin[width_index(vb)] + ko * vb;
                     if (r->vals) memcpy(dst, r->vals, r->n * vb);
                     else memset(dst, 0, r->n * vb);
-                    (vb == 8 ? any_in64 : any_in16) = true;
+                    any_in[width_index(vb)] = true;
                 }
-                if (r->op == PG_OP_QUERY && vb) (vb == 8 ? any_q64 : any_q16) = true;
+                if (r->op == PG_OP_QUERY && vb) any_q[width_index(vb)] = true;
                 st.h_ops[i] = pg_op_desc{te.slot, r->op, ko, r->n};
                 ko += r->n;
             }
             lk.unlock();
             // one copy in, one run per class, one copy out
             cudaMemcpyAsync(st.d_keys, st.h_keys, ko * 8, cudaMemcpyHostToDevice, s->stream);
-            if (any_in64) cudaMemcpyAsync(st.d_vin, st.h_vin, ko * 8, cudaMemcpyHostToDevice, s->stream);
-            if (any_in16) cudaMemcpyAsync(st.d_vin16, st.h_vin16, ko * 2, cudaMemcpyHostToDevice, s->stream);
+            for (int x = 0; x < 3; x++)
+                if (any_in[x])
+                    cudaMemcpyAsync(st.d_vin[x], st.h_vin[x], ko * kWidths[x], cudaMemcpyHostToDevice, s->stream);
             cudaMemcpyAsync(st.d_ops, st.h_ops, reqs.size() * sizeof(pg_op_desc), cudaMemcpyHostToDevice, s->stream);
             cudaMemsetAsync(st.d_counts, 0, reqs.size() * 8, s->stream);
             size_t i = 0;
@@ -278,17 +283,18 @@ void worker_loop(pg_server *s)
                 while (j < reqs.size() && s->tables[reqs[j]->table].cls == cls) j++;
                 st.h_nops[ci] = (uint32_t)(j - i);
                 cudaMemcpyAsync(st.d_nops + ci, st.h_nops + ci, 4, cudaMemcpyHostToDevice, s->stream);
-                const bool w16 = s->classes[cls].vbytes == 2;
+                const int x = width_index(s->classes[cls].vbytes);
                 pg_status rs = pg_batch_run(s->classes[cls].batch, st.d_ops + i, st.d_nops + ci, st.d_keys,
-                                            w16 ? st.d_vin16 : st.d_vin, w16 ? st.d_vout16 : st.d_vout, st.d_flags,
+                                            st.d_vin[x], st.d_vout[x], st.d_flags,
                                             st.d_counts + i, reinterpret_cast<pg_stream_t>(s->stream));
                 if (rs != PG_OK) s->error = rs;
                 i = j;
                 ci++;
             }
             cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->stream);
-            if (any_q64) cudaMemcpyAsync(st.h_vout, st.d_vout, ko * 8, cudaMemcpyDeviceToHost, s->stream);
-            if (any_q16) cudaMemcpyAsync(st.h_vout16, st.d_vout16, ko * 2, cudaMemcpyDeviceToHost, s->stream);
+            for (int x = 0; x < 3; x++)
+                if (any_q[x])
+                    cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->stream);
             cudaMemcpyAsync(st.h_counts, st.d_counts, reqs.size() * 8, cudaMemcpyDeviceToHost, s->stream);
             cudaEventRecord(st.done, s->stream);
             lk.lock();
@@ -330,14 +336,12 @@ pg_status pg_server_create(const pg_server_config *cfg, pg_server **out)
         memset(&st, 0, sizeof(st));
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_keys, K * 8);
         if (e == cudaSuccess) e = cudaMalloc(&st.d_keys, K * 8);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_vin, K * 8);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_vin, K * 8);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_vout, K * 8);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_vout, K * 8);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_vin16, K * 2);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_vin16, K * 2);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_vout16, K * 2);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_vout16, K * 2);
+        for (int x = 0; x < 3; x++) {
+            if (e == cudaSuccess) e = cudaMallocHost(&st.h_vin[x], K * kWidths[x]);
+            if (e == cudaSuccess) e = cudaMalloc(&st.d_vin[x], K * kWidths[x]);
+            if (e == cudaSuccess) e = cudaMallocHost(&st.h_vout[x], K * kWidths[x]);
+            if (e == cudaSuccess) e = cudaMalloc(&st.d_vout[x], K * kWidths[x]);
+        }
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_flags, K);
         if (e == cudaSuccess) e = cudaMalloc(&st.d_flags, K);
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_ops, R * sizeof(pg_op_desc));
@@ -374,14 +378,12 @@ pg_status pg_server_destroy(pg_server *s)
     for (auto &st : s->stages) {
         cudaFreeHost(st.h_keys);
         cudaFree(st.d_keys);
-        cudaFreeHost(st.h_vin);
-        cudaFree(st.d_vin);
-        cudaFreeHost(st.h_vout);
-        cudaFree(st.d_vout);
-        cudaFreeHost(st.h_vin16);
-        cudaFree(st.d_vin16);
-        cudaFreeHost(st.h_vout16);
-        cudaFree(st.d_vout16);
+        for (int x = 0; x < 3; x++) {
+            cudaFreeHost(st.h_vin[x]);
+            cudaFree(st.d_vin[x]);
+            cudaFreeHost(st.h_vout[x]);
+            cudaFree(st.d_vout[x]);
+        }
         cudaFreeHost(st.h_flags);
         cudaFree(st.d_flags);
         cudaFreeHost(st.h_ops);
@@ -402,14 +404,13 @@ pg_status pg_server_destroy(pg_server *s)
 pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t seed, uint32_t *table_id)
 {
     if (!s || !cfg || !table_id) return PG_ERR_INVALID;
-    // staging holds 64- and 16-bit values: the 8-bit bucketed filter is served by the bulk calls only
-    if (cfg->format == PG_FMT_PACKED_TAGVAL8) return PG_ERR_UNSUPPORTED;
     // admission by HBM budget: the table's slot arrays (and fingerprints) must fit
     uint64_t need = 0;
-    const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : 2;
+    const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : cfg->format == PG_FMT_PACKED_TAGVAL8 ? 1 : 2;
     const uint32_t vb = cfg->format == PG_FMT_KV64 ? 8
                         : (cfg->format == PG_FMT_TAGVAL16 || cfg->format == PG_FMT_PACKED_TAGVAL16) ? 2
-                                                                                                    : 0;
+                        : cfg->format == PG_FMT_PACKED_TAGVAL8                                       ? 1
+                                                                                                     : 0;
     for (uint32_t l = 0; l < cfg->nlevels && l < 2; l++) {
         const pg_level_config &L = cfg->levels[l];
         if (L.bucket_size == 0 || L.nslots == 0) return PG_ERR_INVALID;
@@ -489,7 +490,9 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
     if (n > s->cfg.max_wave_keys) return PG_ERR_INVALID;
     std::lock_guard<std::mutex> g(s->mu);
     if (table_id >= s->tables.size() || !s->tables[table_id].live) return PG_ERR_INVALID;
-    if (op == PG_OP_INSERT_WITH_DELETE && s->tables[table_id].t->ifmt != pg::FMT_PACKED16) return PG_ERR_UNSUPPORTED;
+    if (op == PG_OP_INSERT_WITH_DELETE && s->tables[table_id].t->ifmt != pg::FMT_PACKED16 &&
+        s->tables[table_id].t->ifmt != pg::FMT_PACKED8)
+        return PG_ERR_UNSUPPORTED;
     if (s->error != PG_OK) return s->error;
     request *r = new request();
     r->id = s->next_id++;

@@ -130,13 +130,11 @@ def test_server_admits_tables_by_hbm_budget(pg):
 def test_server_serves_bucketed_filters(pg):
     """A 16-bit bucketed filter behind the serving loop: inserts, queries,
     removes and insert_with_delete requests, each result as the table's own
-    bulk call would give it; 8-bit filters are refused."""
+    bulk call would give it."""
     srv = pg.Server(hbm_budget_bytes=1 << 30, max_wave_keys=1 << 16, max_wave_requests=64)
     try:
         tid = srv.add_table(pg.data_structs.del_tcf(1 << 16, 1 << 10), 7)
         assert tid is not None
-        with pytest.raises(pg.PoggersError):
-            srv.add_table(pg.data_structs.del_tcf(1 << 12, 1 << 8, tag_bits=8), 8)
         keys = wl.keys_without_sentinels(21, 40000)
         vals = (wl.values_for(keys, 2, 22).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
         fl = np.zeros(len(keys), dtype=np.uint8)
@@ -155,5 +153,60 @@ def test_server_serves_bucketed_filters(pg):
         fq2 = np.zeros(len(keys), dtype=np.uint8)
         srv.poll(srv.submit(tid, pg.PG_OP_QUERY, keys, None, None, fq2), wait=True)
         assert fq2.all()
+    finally:
+        srv.close()
+
+
+def test_server_serves_8bit_filters_beside_16bit_ones(pg):
+    """An 8-bit and a 16-bit bucketed filter served in the same waves (their
+    values staged at their own widths), against twin tables driven by the bulk
+    calls: every insert and re-add placed, no false negatives, and the 8-bit
+    filter's values agree with its twin's as often as tag collisions allow."""
+    import torch
+    from tests.gpu_util import to_dev
+    srv = pg.Server(hbm_budget_bytes=1 << 30, max_wave_keys=1 << 16, max_wave_requests=64)
+    try:
+        c8 = pg.data_structs.del_tcf(1 << 15, 1 << 9, tag_bits=8)
+        c16 = pg.data_structs.del_tcf(1 << 15, 1 << 9)
+        t8, t16 = srv.add_table(c8, 8), srv.add_table(c16, 16)
+        assert t8 is not None and t16 is not None
+        keys = wl.keys_without_sentinels(31, 24000)
+        v8 = (wl.values_for(keys, 2, 32).astype(np.uint64) & np.uint64(0xFF)).astype(np.uint8)
+        v16 = (wl.values_for(keys, 2, 33).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
+        f8, f16 = np.zeros(len(keys), np.uint8), np.zeros(len(keys), np.uint8)
+        # submitted back to back, so both requests can join one wave
+        r8 = srv.submit(t8, pg.PG_OP_INSERT, keys, v8, None, f8)
+        r16 = srv.submit(t16, pg.PG_OP_INSERT, keys, v16, None, f16)
+        srv.poll(r8, wait=True), srv.poll(r16, wait=True)
+        assert f8.all() and f16.all()
+        q8, q16 = np.zeros(len(keys), np.uint8), np.zeros(len(keys), np.uint16)
+        g8, g16 = np.zeros(len(keys), np.uint8), np.zeros(len(keys), np.uint8)
+        r8 = srv.submit(t8, pg.PG_OP_QUERY, keys, None, q8, g8)
+        r16 = srv.submit(t16, pg.PG_OP_QUERY, keys, None, q16, g16)
+        srv.poll(r8, wait=True), srv.poll(r16, wait=True)
+        assert g8.all() and g16.all()
+        assert (q16 == v16).mean() > 0.999
+        fr = np.zeros(12000, np.uint8)
+        srv.poll(srv.submit(t8, pg.PG_OP_REMOVE, keys[:12000], None, None, fr), wait=True)
+        # a remove takes the first slot with the key's tag, sometimes another key's:
+        # with 8-bit tags a few removes can find none left
+        assert fr.sum() >= 12000 - 10
+        fa = np.zeros(12000, np.uint8)
+        srv.poll(srv.submit(t8, pg.PG_OP_INSERT_WITH_DELETE, keys[:12000], v8[:12000], None, fa), wait=True)
+        assert fa.all()
+
+        # the twin: the same filter through the bulk calls
+        tw = pg.Table(c8, 8)
+        dk = to_dev(keys)
+        ok = torch.zeros(len(keys), dtype=torch.uint8, device="cuda")
+        tw.bulk_insert(dk, torch.from_numpy(v8).cuda(), ok)
+        tv = torch.zeros(len(keys), dtype=torch.uint8, device="cuda")
+        tf = torch.zeros(len(keys), dtype=torch.uint8, device="cuda")
+        tw.bulk_query(dk, tv, tf)
+        torch.cuda.synchronize()
+        assert ok.all() and tf.all()
+        twin_match = (tv.cpu().numpy() == v8).mean()
+        assert abs((q8 == v8).mean() - twin_match) < 0.01, ((q8 == v8).mean(), twin_match)
+        tw.free_on_device()
     finally:
         srv.close()
