@@ -748,18 +748,21 @@ struct level_ops_dyn {
 // evict-last policy so it stays resident while the slots stream past with
 // evict-first.  A probe then reads its bucket's fingerprints from L2 and goes
 // to DRAM only for a slot whose fingerprint matches, reading that 16-byte slot
-// (key and value together); an insert CASes the first empty slot directly.
-// Random DRAM requests per op -- the limit of the plain walk -- drop from
-// ~2.7 per query and ~2.3 per insert at 0.9 load to ~0.55 and ~1.
+// (key and value together).  Random DRAM requests per op -- the limit of the
+// plain walk -- drop from ~2.7 per query and ~2.3 per insert at 0.9 load to
+// ~0.55 and ~0 (an insert only writes its slot).
 //
 // Fingerprint of a slot: 0 empty, 0xFF tombstone (or the key ~0, which the
 // reference cannot tell from one), else 1..254 from the top byte of the
-// key's first hash.  It is written after the key's CAS, so within a phase a
-// snapshot is never fuller than the keys: an insert that trusts it may only
-// lose a CAS race, as with a key snapshot.  The bucket_insert decisions are
-// unchanged: first empty slot for insert; first match at or before the first
-// empty slot for query; first match, then stop at a bucket with an empty
-// non-matching slot, for remove.
+// key's first hash.  An insert claims its slot in the fingerprint array: a
+// CAS on the (L2-resident) fingerprint word holding the bucket's first empty
+// byte sets that byte to the key's fingerprint, and the winner then writes
+// key and value with one 16-byte store.  The claim is the insert's
+// linearisation point, as the key CAS is in the reference; slots are still
+// taken first-empty in slot order, so filled slots stay a prefix of each
+// bucket.  The bucket_insert decisions are unchanged: first empty slot for
+// insert; first match at or before the first empty slot for query; first
+// match, then stop at a bucket with an empty non-matching slot, for remove.
 __device__ __forceinline__ uint64_t l2_policy_evict_last()
 {
     uint64_t p;
@@ -859,6 +862,49 @@ struct level_ops_fp {
         unsigned int *w = reinterpret_cast<unsigned int *>(L.fp + (byte & ~3ULL));
         atomicOr(w, f << (8 * (byte & 3)));
     }
+    // Claim the first empty slot of bucket b (slot order) by setting its
+    // fingerprint byte to f; w is a snapshot of the bucket's fingerprints
+    // (a snapshot is never fuller than the array, fill only grows).  Returns
+    // the slot, or -1 when the bucket is full.  A failed CAS retries on the
+    // word it returned; every failure means a byte of the word changed (0 ->
+    // fingerprint, or fingerprint -> 0xFF on a remove), at most 16 times per
+    // word, so the bound of 64 attempts is never the one that ends the loop.
+    __device__ __forceinline__ static int claim(const level_desc &L, uint64_t b, const uint32_t (&w)[NW], uint32_t f)
+    {
+        if constexpr (B == 4) {
+            unsigned int *p = reinterpret_cast<unsigned int *>(L.fp + b * B);
+            uint32_t old = w[0];
+            for (int it = 0; it < 64; ++it) {
+                const uint32_t e = bytes_eq4(old, 0);
+                if (!e) return -1;
+                const int s = __ffs(e) - 1;
+                const uint32_t prev = atomicCAS(p, old, old | (f << (8 * s)));
+                if (prev == old) return s;
+                old = prev;
+            }
+            return -1;
+        } else {
+#pragma unroll
+            for (int q = 0; q < B / 8; ++q) {
+                unsigned long long *p = reinterpret_cast<unsigned long long *>(L.fp + b * B + 8 * q);
+                unsigned long long old = (unsigned long long)w[2 * q] | ((unsigned long long)w[2 * q + 1] << 32);
+                for (int it = 0; it < 64; ++it) {
+                    const uint32_t e = bytes_eq4((uint32_t)old, 0) | (bytes_eq4((uint32_t)(old >> 32), 0) << 4);
+                    if (!e) break;  // this word is full: the bucket's next word
+                    const int s = __ffs(e) - 1;
+                    const unsigned long long prev = atomicCAS(p, old, old | ((unsigned long long)f << (8 * s)));
+                    if (prev == old) return 8 * q + s;
+                    old = prev;
+                }
+            }
+            return -1;
+        }
+    }
+    // key and value of a claimed slot, one 16-byte store
+    __device__ __forceinline__ static void store_slot(const level_desc &L, uint64_t b, int s, K k, V v)
+    {
+        asm volatile("st.global.v2.u64 [%0], {%1, %2};" ::"l"(slot_key(L, b, s)), "l"(k), "l"(v) : "memory");
+    }
     __device__ __forceinline__ static uint32_t upto(uint32_t e)
     {
         // slots 0 .. first empty (inclusive); all slots when none is empty
@@ -881,16 +927,17 @@ struct level_ops_fp {
             const uint64_t b = L.nbmod.mod(raw);
             uint32_t w[NW];
             load_fp(L, b, w, keep);
-            uint32_t e = match(w, 0);
-            while (e) {
-                const int s = __ffs(e) - 1;
-                if (atomicCAS(slot_key(L, b, s), 0ULL, (K)key) == 0ULL) {
-                    slot_key(L, b, s)[1] = val;
-                    set_fp(L, b, s, f);
-                    return true;
-                }
-                e &= e - 1;
+            const int s = claim(L, b, w, f);
+            if (s < 0) continue;
+            if (f) {
+                store_slot(L, b, s, key, val);
+            } else {
+                // the key 0 (the empty sentinel): as the reference's CAS of 0
+                // over an empty key, it "succeeds" without filling the slot and
+                // writes only the value
+                slot_key(L, b, s)[1] = val;
             }
+            return true;
         }
         return false;
     }
