@@ -216,8 +216,10 @@ def run_ours(args, rank, world):
     achieved = ALGO_BYTES[dom] * dom_units / (dom_ms / 1e3) / 1e9
     tr = traffic_summary()
     traffic = None
-    if tr and dom in tr:
-        traffic = tr[dom]["dram_bytes_per_launch"]
+    # the summary's bytes are per launch of its own key count, for the fingerprint
+    # layout with region-ordered inserts; they scale with the keys of a launch
+    if tr and dom in tr and args.layout == "fingerprints" and args.insert_order == "region":
+        traffic = round(tr[dom]["dram_bytes_per_launch"] * dom_units / tr["keys_per_launch"])
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "Mops/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
