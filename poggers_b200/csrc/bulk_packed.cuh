@@ -16,9 +16,6 @@ struct packed_args {
     uint8_t *found;                 // insert_if_not_exists*: the key was already present
     unsigned long long *count;      // query / remove: successes; insert forms: failures
     uint64_t n;
-    // insert forms over a region-sorted copy of the batch: flags were preset to 1
-    // and only a failure is written, at flags[perm[i]] (the key's place in the caller's batch)
-    const uint32_t *perm;
 };
 
 // build knob: resident blocks the register allocation must allow; 1 measured
@@ -45,10 +42,7 @@ __global__ void __launch_bounds__(256, PG_PACKED_MIN_BLOCKS) k_bulk_packed(table
         bool found = false;
         const bool r = T::op(t, g, OP, key, val, out, found);
         if (g.gl == 0) {
-            if (a.flags) {
-                if (!a.perm) a.flags[i] = (uint8_t)r;
-                else if (!r) a.flags[a.perm[i]] = 0;
-            }
+            if (a.flags) a.flags[i] = (uint8_t)r;
             if constexpr (OP == POP_QUERY || OP == POP_INSERT_IF_NOT_EXISTS || OP == POP_INSERT_IF_NOT_EXISTS_DELETE)
                 if (vout) vout[i] = r ? out : (V)0;
             if constexpr (OP == POP_INSERT_IF_NOT_EXISTS || OP == POP_INSERT_IF_NOT_EXISTS_DELETE)

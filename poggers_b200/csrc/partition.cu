@@ -2,8 +2,9 @@
 // uint64 tables.
 //
 // A random insert into a table much larger than L2 costs a DRAM read for its
-// CAS and a DRAM write-back of the dirty sector, per key: random DRAM
-// transactions are the limit.  Sorting the batch by the table region of each
+// CAS (with fingerprints, a sector the slot store only partly writes) and a
+// DRAM write-back of the dirty sector, per key: random DRAM transactions are
+// the limit.  Sorting the batch by the table region of each
 // key's first bucket (a counting sort into R regions that each fit in L2) lets
 // the insert kernel sweep the table region by region: while the resident
 // threads work through one region, its lines stay in L2, so a line is
@@ -21,7 +22,6 @@
 #include "poggers_b200.h"
 #include "bulk_kernels.cuh"
 #include "table_internal.h"
-#include "bulk_packed.cuh"
 
 namespace pg {
 
@@ -196,11 +196,10 @@ using namespace pg;
 // small for the sort to pay, or no memory for the scratch.
 namespace {
 
-// The region sort shared by the uint64 tables and the bucketed filter: sorts
-// (keys, values of vbytes) into the table's scratch, presets the flags to 1,
-// and returns the sorted copy and the permutation; false when the batch
-// should run in batch order.
-bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&vals, uint32_t vbytes, uint8_t *flags,
+// The region sort: sorts (keys, 8-byte values) into the table's scratch,
+// presets the flags to 1, and returns the sorted copy and the permutation;
+// false when the batch should run in batch order.
+bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&vals, uint8_t *flags,
                  const uint32_t *&perm, cudaStream_t s)
 {
     if (t->bytes[0] < 2 * kPartRegionBytes || n < kPartMinKeys || n >= (1ull << 32)) return false;
@@ -210,7 +209,7 @@ bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&va
     while ((bucket_bytes << (shift + 1)) <= kPartRegionBytes) shift++;
     while (((nb - 1) >> shift) + 1 > kPartMaxRegions) shift++;
     const uint32_t R = (uint32_t)(((nb - 1) >> shift) + 1);
-    // scratch: keys (8 B), values (up to 8 B), original index (4 B) per key; counts and cursors per region
+    // scratch: keys (8 B), values (8 B), original index (4 B) per key; counts and cursors per region
     const uint64_t cnt_off = (n * 20 + 255) & ~255ull;
     const uint64_t need = cnt_off + 2ull * R * 8;
     if (t->part_bytes < need) {
@@ -235,21 +234,8 @@ bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&va
     const region_router route{L, shift};
     k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, R, counts);
     k_part_scan<<<1, 32, 0, s>>>(counts, cursors, R);
-    switch (vbytes) {
-    case 2:
-        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned short *>(vals), n, R,
-                                                     cursors, okeys, static_cast<unsigned short *>(ovals), operm);
-        break;
-    case 1:
-        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned char *>(vals), n, R,
-                                                     cursors, okeys, static_cast<unsigned char *>(ovals), operm);
-        break;
-    default:
-        k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned long long *>(vals), n,
-                                                     R, cursors, okeys, static_cast<unsigned long long *>(ovals),
-                                                     operm);
-        break;
-    }
+    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned long long *>(vals), n, R,
+                                                 cursors, okeys, static_cast<unsigned long long *>(ovals), operm);
     if (flags) cudaMemsetAsync(flags, 1, n, s);
     keys = okeys;
     vals = ovals;
@@ -263,16 +249,7 @@ bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
 {
     const bool kv64 = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT || t->ifmt == FMT_KV64_FP;
     if (!t->partition || !kv64 || t->cfg.levels[0].scheme != PG_SCHEME_BUCKET || t->max_blocks == 1) return false;
-    return region_sort(t, a.n, a.keys, a.vals_in, 8, a.flags, a.perm, s);
-}
-
-// The bucketed filter's inserts: the first probe of both of its schemes is
-// bucket MurmurHash64A(key, seed) % nb, the bucket the regions are cut by.
-bool pg_partition_packed(pg_table *t, packed_args &a, cudaStream_t s)
-{
-    const bool packed = t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8;
-    if (!t->partition || !packed || t->max_blocks == 1) return false;
-    return region_sort(t, a.n, a.keys, a.vals_in, t->ifmt == FMT_PACKED16 ? 2u : 1u, a.flags, a.perm, s);
+    return region_sort(t, a.n, a.keys, a.vals_in, a.flags, a.perm, s);
 }
 
 // ---------------------------------------------------------------- sharding

@@ -382,7 +382,6 @@ pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals
 {
     if (t && packed(t->cfg.format)) {
         packed_args p{d_keys, d_vals, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_fail_count), n};
-        if (d_keys && n) pg_partition_packed(t, p, reinterpret_cast<cudaStream_t>(stream));
         return run_packed(t, POP_INSERT, p, stream);
     }
     bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
@@ -418,7 +417,6 @@ pg_status pg_bulk_insert_with_delete(pg_table *t, const uint64_t *d_keys, const 
                                      uint8_t *d_ok, uint64_t *d_fail_count, pg_stream_t stream)
 {
     packed_args p{d_keys, d_vals, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_fail_count), n};
-    if (t && packed(t->cfg.format) && d_keys && n) pg_partition_packed(t, p, reinterpret_cast<cudaStream_t>(stream));
     return run_packed(t, POP_INSERT_DELETE, p, stream);
 }
 

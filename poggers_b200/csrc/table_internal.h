@@ -26,8 +26,6 @@ struct pg_table {
 
 uint32_t pg_table_lanes(const pg_table *t);
 
-namespace pg { struct bulk_args; struct packed_args; }
+namespace pg { struct bulk_args; }
 // Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted copy.
 bool pg_partition_insert(pg_table *t, pg::bulk_args &a, cudaStream_t s);
-// Region-ordered insert / insert_with_delete of the bucketed filter.
-bool pg_partition_packed(pg_table *t, pg::packed_args &a, cudaStream_t s);

@@ -99,40 +99,27 @@ def test_small_batches_take_the_unordered_path(pg):
 
 
 @pytest.mark.parametrize("bits", [16, 8])
-def test_ordered_insert_of_bucketed_filter(pg, bits):
-    """The bucketed filter's insert and insert_with_delete on a region-sorted
-    batch (a 2^25-slot primary level: 128 MiB at 16-bit tags): every key
-    placed, found, its flag at its own batch position; fills equal the
-    unordered run's; re-adds through insert_with_delete likewise."""
+def test_bucketed_filter_keeps_batch_order(pg, bits):
+    """The bucketed filter is never region-sorted: with region ordering on, a
+    large insert at 0.9 load allocates no scratch and sends as many keys to the
+    1 % backing level as with it off.  (Sorting by the first choice would
+    unbalance the two choices, about 5x the keys reaching the backing level,
+    and would change which keys the linear level displaces, which its
+    live-fill stop rule makes visible to later removes.)"""
     from tests.test_bucketed_gpu import _run
     n0 = 1 << 25 if bits == 16 else 1 << 26
-    n1 = n0 // 100
-    n = 3 << 20
-    keys = wl.keys_without_sentinels(71, n)
-    mask = (1 << bits) - 1
-    vals = wl.values_for(keys, 2, 72).astype(np.uint64) & np.uint64(mask)
-    runs = []
+    n = int(0.9 * n0)
+    keys = wl.keys_without_sentinels(73, n)
+    vals = wl.values_for(keys, 2, 74).astype(np.uint64) & np.uint64((1 << bits) - 1)
+    backing = []
     for part in (True, False):
-        t = pg.Table(pg.data_structs.del_tcf(n0, n1, tag_bits=bits), 5)
+        t = pg.Table(pg.data_structs.del_tcf(n0, n0 // 100, tag_bits=bits), 5)
         t.set_partitioned_insert(part)
+        before = t.host_bytes_in_use()
         ok, _, _ = _run(pg, t, bits, 0, keys, vals)
-        f, v, _ = _run(pg, t, bits, 1, keys)
-        r, _, _ = _run(pg, t, bits, 2, keys[: n // 2])
-        a, _, _ = _run(pg, t, bits, 3, keys[: n // 2], vals[: n // 2])
-        fills = [t.get_fill(0), t.get_fill(1)]
-        runs.append((ok, f, v, r, a, fills, t.host_bytes_in_use()))
-    (ok1, f1, v1, r1, a1, fl1, b1), (ok2, f2, v2, r2, a2, fl2, b2) = runs
-    assert ok1.all() and ok2.all() and f1.all() and f2.all() and a1.all() and a2.all()
-    assert b1 > b2  # the sort's scratch belongs to the table
-    def live(fl):
-        return sum(o - t for o, t in fl)
-    assert live(fl1) == n - int(r1.sum()) + int(a1.sum())
-    assert live(fl2) == n - int(r2.sum()) + int(a2.sum())
-    assert abs(int(r1.sum()) - int(r2.sum())) <= 10
-    # a shared tag answers with the value of whichever key holds the earlier slot:
-    # both orders show the same collision rate
-    m1, m2 = (v1 != vals).mean(), (v2 != vals).mean()
-    if bits == 16:
-        assert m1 < 0.001 and m2 < 0.001
-    else:
-        assert abs(m1 - m2) <= 0.2 * max(m1, m2) + 0.001
+        _run(pg, t, bits, 2, keys[:1 << 21])
+        a, _, _ = _run(pg, t, bits, 3, keys[:1 << 21], vals[:1 << 21])
+        assert ok.all() and a.all() and t.host_bytes_in_use() == before
+        backing.append(t.get_fill(1)[0])
+        t.free_on_device()
+    assert abs(backing[0] - backing[1]) <= max(500, backing[1] // 10), backing
