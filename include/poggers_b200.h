@@ -148,9 +148,11 @@ uint64_t pg_table_bytes(const pg_table *t);
 
 /* Launch shape of the bulk kernels: threads per block (<= 256, a multiple of
  * the lanes per key; 0 = 256), blocks per SM (0 = 32), a cap on blocks (0 =
- * none) and the lanes that serve one key (0 = the config's tile; 1, 2, 4, 8
- * or 16, at most the level-0 bucket size; packed formats run 1 or 4 lanes and
- * start at 1).  The lanes per key never change a
+ * none) and the lanes that serve one key (1, 2, 4, 8 or 16, at most the
+ * level-0 bucket size; packed formats run 1 or 4 lanes).  Lanes 0, the
+ * default of a new table, chooses them per operation by measurement: one
+ * lane per key, except two for queries and removes of uint64 tables without
+ * fingerprints.  The lanes per key never change a
  * result: filled slots always form a prefix of each bucket, so the
  * reference's tile-wide stripes decide exactly what a whole-bucket scan
  * decides.  block_threads == lanes with max_blocks == 1 runs the batch

@@ -110,14 +110,12 @@ pg_status cuda_status(cudaError_t e)
     return PG_ERR_CUDA;
 }
 
-uint32_t lanes_of(const pg_table *t) { return pg_table_lanes(t); }
-
 // ordered: one group per key with no wrap-around (a region-ordered batch), so
 // the resident blocks always cover one contiguous window of the batch
-void launch_shape(const pg_table *t, uint64_t n, dim3 &grid, dim3 &block, bool ordered = false)
+void launch_shape(const pg_table *t, uint32_t lanes, uint64_t n, dim3 &grid, dim3 &block, bool ordered = false)
 {
     const uint32_t bt = t->block_threads;
-    const uint64_t groups_per_block = bt / lanes_of(t);
+    const uint64_t groups_per_block = bt / lanes;
     uint64_t need = (n + groups_per_block - 1) / groups_per_block;
     uint64_t cap = ordered ? 0x7fffffffull : (uint64_t)t->num_sms * t->blocks_per_sm;
     if (t->max_blocks && cap > t->max_blocks) cap = t->max_blocks;
@@ -133,9 +131,10 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     if (a.n == 0) return PG_OK;
     if (!a.keys) return PG_ERR_INVALID;
     dim3 grid, block;
-    launch_shape(t, a.n, grid, block, a.perm != nullptr);
+    const uint32_t tile = pg_table_lanes(t, op);
+    launch_shape(t, tile, a.n, grid, block, a.perm != nullptr);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const uint32_t b0 = t->cfg.levels[0].bucket_size, tile = lanes_of(t);
+    const uint32_t b0 = t->cfg.levels[0].bucket_size;
     const table_desc &d = t->desc;
     cudaError_t e;
     switch (t->ifmt) {
@@ -160,10 +159,10 @@ pg_status run_packed(pg_table *t, int op, const packed_args &a, pg_stream_t stre
     // launch: with deletes in the mix, which of two keys sharing a tag holds the
     // earlier slot (and so which one a remove takes) follows the batch order
     dim3 grid, block;
-    launch_shape(t, a.n, grid, block, true);
+    const uint32_t lanes = pg_table_lanes(t, op);
+    launch_shape(t, lanes, a.n, grid, block, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t b0 = t->cfg.levels[0].bucket_size, b1 = t->cfg.nlevels > 1 ? t->cfg.levels[1].bucket_size : 8;
-    const uint32_t lanes = lanes_of(t);
     const cudaError_t e = t->ifmt == FMT_PACKED16 ? launch_packed16(op, b0, b1, lanes, t->desc, a, grid, block, s)
                                                   : launch_packed8(op, b0, b1, lanes, t->desc, a, grid, block, s);
     return cuda_status(e);
@@ -212,12 +211,18 @@ __global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, u
 
 }  // namespace
 
-// lanes a kernel uses per key for this table
-uint32_t pg_table_lanes(const pg_table *t)
+// Lanes per key for one operation.  Unless pg_table_set_launch fixed them,
+// the fastest measured on B200 (2^22-2^30 slots, 0.85-0.9 load): one lane
+// per key, which loads the whole bucket itself, except two for queries and
+// removes of uint64 tables without fingerprints, whose 128-byte buckets two
+// lanes scan faster (16.6 vs 10.1 G queries/s at 8-slot buckets; inserts
+// 17.6 vs 13.0 G/s the other way).  The lanes never change a result.
+uint32_t pg_table_lanes(const pg_table *t, int op)
 {
-    if (t->ifmt == FMT_KV64_FP) return 1u;  // the fingerprint walk serves a key with one lane
     if (t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8) return t->lanes >= 4 ? 4u : 1u;  // compiled widths
-    return t->lanes;
+    if (t->lanes) return t->lanes;
+    const bool kv = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT;
+    return kv && op != OP_INSERT && t->block_threads % 2 == 0 ? 2u : 1u;
 }
 
 extern "C" {
@@ -258,9 +263,8 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
     t->block_threads = 256;
     t->blocks_per_sm = 32;
     t->max_blocks = 0;
-    // packed buckets: one lane reads a whole 64-byte bucket in one go and measured
-    // fastest (the lanes never change a result); otherwise the config's tile
-    t->lanes = packed(cfg->format) ? 1u : cfg->tile;
+    // lanes per key chosen per operation (pg_table_lanes) until set_launch fixes them
+    t->lanes = 0;
     t->partition = 1;
     t->ifmt = internal_format(cfg);
     t->desc.nlevels = cfg->nlevels;
@@ -361,14 +365,13 @@ pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t bloc
                               uint32_t lanes_per_key)
 {
     if (!t) return PG_ERR_INVALID;
-    if (lanes_per_key == 0) lanes_per_key = t->cfg.tile;
-    if (!(lanes_per_key == 1 || lanes_per_key == 2 || lanes_per_key == 4 || lanes_per_key == 8 ||
-          lanes_per_key == 16))
+    if (!(lanes_per_key == 0 || lanes_per_key == 1 || lanes_per_key == 2 || lanes_per_key == 4 ||
+          lanes_per_key == 8 || lanes_per_key == 16))
         return PG_ERR_INVALID;
     if (lanes_per_key > t->cfg.levels[0].bucket_size) return PG_ERR_UNSUPPORTED;
     if (block_threads == 0) block_threads = 256;
     if (blocks_per_sm == 0) blocks_per_sm = 32;
-    if (block_threads > 256 || block_threads % lanes_per_key != 0) return PG_ERR_INVALID;
+    if (block_threads > 256 || (lanes_per_key && block_threads % lanes_per_key != 0)) return PG_ERR_INVALID;
     if (block_threads < 32 && max_blocks != 1) return PG_ERR_INVALID;  // partial warps only for the serial shape
     t->lanes = lanes_per_key;
     t->block_threads = block_threads;

@@ -17,14 +17,15 @@ struct pg_table {
     uint32_t block_threads;
     uint32_t blocks_per_sm;
     uint32_t max_blocks;
-    uint32_t lanes;  // lanes per key used by the kernels (defaults to the config's tile)
+    uint32_t lanes;  // lanes per key set by pg_table_set_launch; 0 = chosen per operation (pg_table_lanes)
     uint32_t ifmt;  // internal format: public format, split variant when PG_TABLE_SPLIT_BUCKETS
     uint32_t partition;  // region-ordered inserts enabled
     void *part_buf;      // their scratch (keys, values, original index, region counts)
     uint64_t part_bytes;
 };
 
-uint32_t pg_table_lanes(const pg_table *t);
+// lanes per key the kernels use for one operation (0 insert, 1 query, 2 remove)
+uint32_t pg_table_lanes(const pg_table *t, int op = 1);
 
 namespace pg { struct bulk_args; }
 // Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted copy.
