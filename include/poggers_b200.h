@@ -152,7 +152,9 @@ uint64_t pg_table_bytes(const pg_table *t);
  * level-0 bucket size; packed formats run 1 or 4 lanes).  Lanes 0, the
  * default of a new table, chooses them per operation by measurement: one
  * lane per key, except two for queries and removes of uint64 tables without
- * fingerprints.  The lanes per key never change a
+ * fingerprints, and four (the reference's tile) for inserts into a
+ * two-choice level of fewer than 2^18 slots, where one lane per key puts the
+ * whole batch in flight at once and unbalances the two choices.  The lanes per key never change a
  * result: filled slots always form a prefix of each bucket, so the
  * reference's tile-wide stripes decide exactly what a whole-bucket scan
  * decides.  block_threads == lanes with max_blocks == 1 runs the batch

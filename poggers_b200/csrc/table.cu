@@ -216,11 +216,21 @@ __global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, u
 // per key, which loads the whole bucket itself, except two for queries and
 // removes of uint64 tables without fingerprints, whose 128-byte buckets two
 // lanes scan faster (16.6 vs 10.1 G queries/s at 8-slot buckets; inserts
-// 17.6 vs 13.0 G/s the other way).  The lanes never change a result.
+// 17.6 vs 13.0 G/s the other way).  The lanes never change a sequential
+// result; they do change how many keys run at once.  Inserts into a
+// two-choice level of fewer than 2^18 slots take 4 lanes, the reference's
+// tile: at one lane the whole batch is in flight together, the shortcut's
+// fill checks see stale counts and keys pile into their first choice (a
+// 2^16-slot TCF with 1 % backing at 0.9 load failed ~800 keys at one lane,
+// ~100 in the reference's own build, none at 4 lanes).
 uint32_t pg_table_lanes(const pg_table *t, int op)
 {
     if (t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8) return t->lanes >= 4 ? 4u : 1u;  // compiled widths
     if (t->lanes) return t->lanes;
+    const pg_level_config &L0 = t->cfg.levels[0];
+    if (op == OP_INSERT && L0.scheme == PG_SCHEME_TWO_CHOICE && L0.nslots < (1ull << 18) &&
+        t->block_threads % 4 == 0 && L0.bucket_size >= 4)
+        return 4u;
     const bool kv = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT;
     return kv && op != OP_INSERT && t->block_threads % 2 == 0 ? 2u : 1u;
 }
