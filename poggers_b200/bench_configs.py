@@ -550,7 +550,7 @@ def config5(args):
                              "queries": n, "query_mops_e2e": round(n / el_q / 1e6, 1),
                              "query_p50_ms": round(1e3 * float(np.percentile(lat_q, 50)), 2),
                              "query_p99_ms": round(1e3 * float(np.percentile(lat_q, 99)), 2),
-                             "note": "host numpy buffers in, values out: PCIe-bound end to end"}
+                             "note": "host numpy buffers in, values out; per wave: host copies into pinned staging (split over threads), PCIe transfers and kernels, two waves in flight"}
     return res
 
 

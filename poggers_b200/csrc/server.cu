@@ -57,6 +57,7 @@ struct table_entry {
     uint32_t slot;     // index in its class's batch
     uint64_t bytes;
     bool live;
+    uint32_t inflight = 0;  // requests taken into a wave and not yet completed
 };
 
 struct klass {
@@ -173,20 +174,82 @@ std::vector<request *> take_wave(pg_server *s, pg_server::stage &st, uint64_t &n
     return out;
 }
 
-void complete_stage(pg_server *s, pg_server::stage &st, std::vector<request *> &reqs, uint64_t *key_off)
+// One host copy into or out of the pinned staging buffers; src == nullptr
+// zero-fills.
+struct copy_job {
+    void *dst;
+    const void *src;
+    uint64_t bytes;
+};
+
+// Run the copies of one wave.  A single thread's memcpy moves a fraction of
+// what host memory and the PCIe link take, so a wave of more than 8 MB is
+// split into equal byte ranges over up to 8 threads (half the host's
+// hardware threads at most).
+void copy_all(const std::vector<copy_job> &jobs)
 {
-    // copy results out of the pinned staging buffers into the clients' buffers
-    uint32_t i = 0;
-    for (request *r : reqs) {
-        const uint64_t o = key_off[i];
-        const table_entry &te = s->tables[r->table];
-        const uint32_t vb = s->classes[te.cls].vbytes;
-        if (r->flags) memcpy(r->flags, st.h_flags + o, r->n);
-        if (r->op == PG_OP_QUERY && r->vals_out && vb)
-            memcpy(r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb);
-        r->count = st.h_counts[i];
-        r->t_done = now_s();
-        i++;
+    uint64_t total = 0;
+    for (const copy_job &j : jobs) total += j.bytes;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned nt = total < (8ull << 20) ? 1u : std::max(1u, std::min(8u, hw / 2));
+    auto part = [&](unsigned k) {
+        const uint64_t lo = total * k / nt, hi = total * (k + 1) / nt;
+        uint64_t at = 0;
+        for (const copy_job &j : jobs) {
+            const uint64_t a = std::max(lo, at), b = std::min(hi, at + j.bytes);
+            if (a < b) {
+                char *d = static_cast<char *>(j.dst) + (a - at);
+                if (j.src) memcpy(d, static_cast<const char *>(j.src) + (a - at), b - a);
+                else memset(d, 0, b - a);
+            }
+            at += j.bytes;
+            if (at >= hi) break;
+        }
+    };
+    if (nt == 1) {
+        part(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned k = 1; k < nt; k++) th.emplace_back(part, k);
+    part(0);
+    for (std::thread &t : th) t.join();
+}
+
+// What a wave's copies and launches need from the server's tables, read
+// while the lock is held: client threads may add tables meanwhile, which
+// can move the table and class arrays.
+struct wave_plan {
+    std::vector<request *> reqs;
+    std::vector<uint64_t> key_off;  // each request's first key in the staging buffers
+    std::vector<uint32_t> vb;       // value bytes of its table
+    std::vector<uint32_t> slot;     // its table's index in the class batch
+    struct run {
+        pg_batch *batch;
+        uint32_t first, count, vb;
+    };
+    std::vector<run> runs;  // one pg_batch_run per kernel class, requests [first, first + count)
+    uint64_t nkeys = 0;
+};
+
+// Copy a finished wave's results out of the pinned staging buffers into the
+// clients' buffers (without the lock: the requests belong to the worker until
+// they are published).
+void complete_stage(pg_server::stage &st, const wave_plan &pl)
+{
+    std::vector<copy_job> jobs;
+    for (size_t i = 0; i < pl.reqs.size(); i++) {
+        request *r = pl.reqs[i];
+        const uint64_t o = pl.key_off[i];
+        const uint32_t vb = pl.vb[i];
+        if (r->flags) jobs.push_back({r->flags, st.h_flags + o, r->n});
+        if (r->op == PG_OP_QUERY && r->vals_out && vb) jobs.push_back({r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb});
+    }
+    copy_all(jobs);
+    const double t = now_s();
+    for (size_t i = 0; i < pl.reqs.size(); i++) {
+        pl.reqs[i]->count = st.h_counts[i];
+        pl.reqs[i]->t_done = t;
     }
 }
 
@@ -194,8 +257,7 @@ void worker_loop(pg_server *s)
 {
     cudaSetDevice(s->device);
     struct slot_state {
-        std::vector<request *> reqs;
-        std::vector<uint64_t> key_off;
+        wave_plan plan;
         bool busy = false;
     } slots[kMaxWaves];
     int next_slot = 0;
@@ -207,9 +269,14 @@ void worker_loop(pg_server *s)
             int w = (next_slot + k) % kMaxWaves;
             if (!slots[w].busy) continue;
             if (cudaEventQuery(s->stages[w].done) == cudaSuccess) {
-                complete_stage(s, s->stages[w], slots[w].reqs, slots[w].key_off.data());
-                for (request *r : slots[w].reqs) s->done[r->id] = r;
-                slots[w].reqs.clear();
+                lk.unlock();
+                complete_stage(s->stages[w], slots[w].plan);
+                lk.lock();
+                for (request *r : slots[w].plan.reqs) {
+                    s->tables[r->table].inflight--;
+                    s->done[r->id] = r;
+                }
+                slots[w].plan = wave_plan();
                 slots[w].busy = false;
                 progressed = true;
             }
@@ -243,62 +310,72 @@ void worker_loop(pg_server *s)
             uint64_t nkeys;
             uint32_t nops;
             std::vector<uint32_t> opc;
-            std::vector<request *> reqs = take_wave(s, st, nkeys, nops, opc);
+            wave_plan &pl = slots[w].plan;
+            pl.reqs = take_wave(s, st, nkeys, nops, opc);
             // group requests by class; each class's requests are contiguous in the op array
-            std::stable_sort(reqs.begin(), reqs.end(), [&](request *a, request *b) {
+            std::stable_sort(pl.reqs.begin(), pl.reqs.end(), [&](request *a, request *b) {
                 return s->tables[a->table].cls < s->tables[b->table].cls;
             });
-            slots[w].key_off.assign(reqs.size(), 0);
+            const size_t nr = pl.reqs.size();
+            pl.key_off.assign(nr, 0);
+            pl.vb.assign(nr, 0);
+            pl.slot.assign(nr, 0);
             uint64_t ko = 0;
+            for (size_t i = 0; i < nr; i++) {
+                table_entry &te = s->tables[pl.reqs[i]->table];
+                te.inflight++;
+                pl.key_off[i] = ko;
+                pl.vb[i] = s->classes[te.cls].vbytes;
+                pl.slot[i] = te.slot;
+                ko += pl.reqs[i]->n;
+                if (i == 0 || te.cls != s->tables[pl.reqs[i - 1]->table].cls)
+                    pl.runs.push_back({s->classes[te.cls].batch, (uint32_t)i, 0, s->classes[te.cls].vbytes});
+                pl.runs.back().count++;
+            }
+            pl.nkeys = ko;
+            lk.unlock();
+            // stage keys and values in pinned memory
+            std::vector<copy_job> jobs;
             bool any_in[3] = {false, false, false}, any_q[3] = {false, false, false};
-            for (size_t i = 0; i < reqs.size(); i++) {
-                request *r = reqs[i];
-                const table_entry &te = s->tables[r->table];
-                const uint32_t vb = s->classes[te.cls].vbytes;
-                slots[w].key_off[i] = ko;
-                memcpy(st.h_keys + ko, r->keys, r->n * 8);
+            for (size_t i = 0; i < nr; i++) {
+                request *r = pl.reqs[i];
+                const uint64_t o = pl.key_off[i];
+                const uint32_t vb = pl.vb[i];
+                jobs.push_back({st.h_keys + o, r->keys, r->n * 8});
                 if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
-                    unsigned char *dst = st.h_vin[width_index(vb)] + ko * vb;
-                    if (r->vals) memcpy(dst, r->vals, r->n * vb);
-                    else memset(dst, 0, r->n * vb);
+                    jobs.push_back({st.h_vin[width_index(vb)] + o * vb, r->vals, r->n * vb});
                     any_in[width_index(vb)] = true;
                 }
                 if (r->op == PG_OP_QUERY && vb) any_q[width_index(vb)] = true;
-                st.h_ops[i] = pg_op_desc{te.slot, r->op, ko, r->n};
-                ko += r->n;
+                st.h_ops[i] = pg_op_desc{pl.slot[i], r->op, o, r->n};
             }
-            lk.unlock();
+            copy_all(jobs);
             // one copy in, one run per class, one copy out
             cudaMemcpyAsync(st.d_keys, st.h_keys, ko * 8, cudaMemcpyHostToDevice, s->stream);
             for (int x = 0; x < 3; x++)
                 if (any_in[x])
                     cudaMemcpyAsync(st.d_vin[x], st.h_vin[x], ko * kWidths[x], cudaMemcpyHostToDevice, s->stream);
-            cudaMemcpyAsync(st.d_ops, st.h_ops, reqs.size() * sizeof(pg_op_desc), cudaMemcpyHostToDevice, s->stream);
-            cudaMemsetAsync(st.d_counts, 0, reqs.size() * 8, s->stream);
-            size_t i = 0;
-            uint32_t ci = 0;
-            while (i < reqs.size()) {
-                const uint32_t cls = s->tables[reqs[i]->table].cls;
-                size_t j = i;
-                while (j < reqs.size() && s->tables[reqs[j]->table].cls == cls) j++;
-                st.h_nops[ci] = (uint32_t)(j - i);
+            cudaMemcpyAsync(st.d_ops, st.h_ops, nr * sizeof(pg_op_desc), cudaMemcpyHostToDevice, s->stream);
+            cudaMemsetAsync(st.d_counts, 0, nr * 8, s->stream);
+            pg_status launch_error = PG_OK;
+            for (size_t ci = 0; ci < pl.runs.size(); ci++) {
+                const wave_plan::run &rn = pl.runs[ci];
+                st.h_nops[ci] = rn.count;
                 cudaMemcpyAsync(st.d_nops + ci, st.h_nops + ci, 4, cudaMemcpyHostToDevice, s->stream);
-                const int x = width_index(s->classes[cls].vbytes);
-                pg_status rs = pg_batch_run(s->classes[cls].batch, st.d_ops + i, st.d_nops + ci, st.d_keys,
-                                            st.d_vin[x], st.d_vout[x], st.d_flags,
-                                            st.d_counts + i, reinterpret_cast<pg_stream_t>(s->stream));
-                if (rs != PG_OK) s->error = rs;
-                i = j;
-                ci++;
+                const int x = width_index(rn.vb);
+                pg_status rs = pg_batch_run(rn.batch, st.d_ops + rn.first, st.d_nops + ci, st.d_keys, st.d_vin[x],
+                                            st.d_vout[x], st.d_flags, st.d_counts + rn.first,
+                                            reinterpret_cast<pg_stream_t>(s->stream));
+                if (rs != PG_OK) launch_error = rs;
             }
             cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->stream);
             for (int x = 0; x < 3; x++)
                 if (any_q[x])
                     cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->stream);
-            cudaMemcpyAsync(st.h_counts, st.d_counts, reqs.size() * 8, cudaMemcpyDeviceToHost, s->stream);
+            cudaMemcpyAsync(st.h_counts, st.d_counts, nr * 8, cudaMemcpyDeviceToHost, s->stream);
             cudaEventRecord(st.done, s->stream);
             lk.lock();
-            slots[w].reqs = std::move(reqs);
+            if (launch_error != PG_OK) s->error = launch_error;
             slots[w].busy = true;
             s->waves_run++;
             s->keys_run += ko;
@@ -346,8 +423,8 @@ pg_status pg_server_create(const pg_server_config *cfg, pg_server **out)
         if (e == cudaSuccess) e = cudaMalloc(&st.d_flags, K);
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_ops, R * sizeof(pg_op_desc));
         if (e == cudaSuccess) e = cudaMalloc(&st.d_ops, R * sizeof(pg_op_desc));
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_nops, 64 * 4);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_nops, 64 * 4);
+        if (e == cudaSuccess) e = cudaMallocHost(&st.h_nops, R * 4);  // one run per class, at most one per request
+        if (e == cudaSuccess) e = cudaMalloc(&st.d_nops, R * 4);
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_counts, R * 8);
         if (e == cudaSuccess) e = cudaMalloc(&st.d_counts, R * 8);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming);
@@ -457,6 +534,7 @@ pg_status pg_server_drop_table(pg_server *s, uint32_t table_id)
     if (table_id >= s->tables.size() || !s->tables[table_id].live) return PG_ERR_INVALID;
     for (request *r : s->pending)
         if (r->table == table_id) return PG_ERR_INVALID;  // collect its requests first
+    if (s->tables[table_id].inflight) return PG_ERR_INVALID;  // and those already in a wave
     table_entry &te = s->tables[table_id];
     te.live = false;
     klass &k = s->classes[te.cls];

@@ -210,3 +210,37 @@ def test_server_serves_8bit_filters_beside_16bit_ones(pg):
         tw.free_on_device()
     finally:
         srv.close()
+
+
+def test_server_large_requests_split_their_host_copies(pg):
+    """Requests of 2^21 keys (16 MiB of keys and as much of values, so the
+    wave's host copies are split over several threads) on a uint64 table with
+    fingerprints: every insert placed, every query answered with its value,
+    absent keys not found, removes seen by the next query; the table dropped
+    afterwards."""
+    srv = pg.Server(hbm_budget_bytes=4 << 30, max_wave_keys=1 << 22, max_wave_requests=64)
+    try:
+        cfg = pg.data_structs.hash_table_64(1 << 23, bucket=8)
+        cfg.fingerprints = True
+        tid = srv.add_table(cfg, 9)
+        n = 1 << 21
+        keys = wl.keys_without_sentinels(81, n)
+        vals = wl.values_for(keys, 8, 82)
+        fl = np.zeros(n, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_INSERT, keys, vals, None, fl), wait=True)
+        assert fl.all()
+        q = np.concatenate([keys[: n // 2], wl.keys_without_sentinels(83, n // 2)])
+        vo = np.zeros(n, dtype=np.uint64)
+        fq = np.zeros(n, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_QUERY, q, None, vo, fq), wait=True)
+        assert fq[: n // 2].all() and not fq[n // 2:].any()
+        assert (vo[: n // 2] == vals[: n // 2]).all() and (vo[n // 2:] == 0).all()
+        fr = np.zeros(n // 4, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_REMOVE, keys[: n // 4], None, None, fr), wait=True)
+        assert fr.all()
+        fq2 = np.zeros(n // 2, dtype=np.uint8)
+        srv.poll(srv.submit(tid, pg.PG_OP_QUERY, keys[: n // 2], None, None, fq2), wait=True)
+        assert not fq2[: n // 4].any() and fq2[n // 4:].all()
+        srv.drop_table(tid)
+    finally:
+        srv.close()
