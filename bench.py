@@ -203,8 +203,9 @@ def run_ours(args, rank, world):
 
     e2e = None if args.no_e2e else run_e2e(args, table, keys, vals, qkeys, dev, world)
 
-    # per step: the insert kernel (after the region count, scan and scatter kernels
-    # when the batch is region-ordered) and the query kernel; clears are memsets
+    # per step: the insert kernel (after the run bases and scatter kernels, and
+    # followed by the pass for keys that missed their run, when the batch is
+    # region-ordered) and the query kernel; clears are memsets
     ordered = args.insert_order == "region" and n >= (1 << 20) and NSLOTS * 16 >= (64 << 20)
     launches_per_step = (4 if ordered else 1) + 1
     ops = (n + nq) * args.steps * world

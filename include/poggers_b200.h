@@ -187,11 +187,14 @@ pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t
 
 /* Region-ordered inserts (on by default; enable = 0 turns them off).  A
  * batch of at least 2^20 keys into a uint64 bucket table of at least 64 MB
- * is first counting-sorted by the table region (32 MB) of each key's first
- * bucket, then inserted in that order, so each bucket line is fetched from
- * HBM once for all its keys instead of once per key.  The sort costs 20
- * bytes of device scratch per key, allocated by the first such insert and
- * kept by the table (counted in pg_table_bytes) until pg_table_destroy.
+ * is first sorted by the table region (32 MB) of each key's first bucket,
+ * into one run per region, then inserted in that order, so each bucket line
+ * is fetched from HBM once for all its keys instead of once per key.  A run
+ * holds the keys expected in its region plus a margin; the keys a run cannot
+ * hold (a batch far from uniform over the table) are inserted afterwards in
+ * batch order.  The sort costs about 20 bytes of device scratch per key,
+ * allocated by the first such insert and kept by the table (counted in
+ * pg_table_bytes) until pg_table_destroy.
  * Concurrent inserts have no defined order in the reference either: which
  * keys fail when a table overflows may differ, every placed key is
  * placed by the same rule.  The scratch is the table's: two region-ordered

@@ -24,6 +24,14 @@ struct bulk_args {
     // insert over a permuted copy of the batch: flags were preset to 1 and only
     // a failure is written, at flags[perm[i]] (the key's place in the caller's batch)
     const uint32_t *perm;
+    // the permuted copy in runs of region_cap entries, one run per table region:
+    // run r holds region_cursor[r] - r * region_cap keys (at most region_cap),
+    // the rest of the run is unused; region_div = 2^64 / region_cap rounded up,
+    // so that i / region_cap = mulhi(region_div, i) for i < 2^32
+    const unsigned long long *region_cursor;
+    uint64_t region_cap, region_div;
+    // insert only the keys whose bit is set (those that did not fit their run)
+    const uint32_t *only;
 };
 
 __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
@@ -61,7 +69,34 @@ __global__ void __launch_bounds__(256, min_blocks_of<FMT>()) k_bulk(table_desc t
     const V *vin = static_cast<const V *>(a.vals_in);
     V *vout = static_cast<V *>(a.vals_out);
     uint32_t c = 0;
+    if constexpr (OP == OP_INSERT) {
+        if (a.only) {
+            // the keys a region-sorted pass could not place in their runs, in batch order
+            const uint64_t nw = (a.n + 31) / 32;
+            for (uint64_t w = gid; w < nw; w += ngroups) {
+                uint32_t bits = __ldg(a.only + w);
+                while (bits) {
+                    const uint64_t i = w * 32 + (uint64_t)(__ffs(bits) - 1);
+                    bits &= bits - 1;
+                    const bool r = T::insert(t, g, __ldg(a.keys + i), vin ? __ldg(vin + i) : (V)0);
+                    if (g.gl == 0) {
+                        if (a.flags) a.flags[i] = (uint8_t)r;
+                        c += !r;
+                    }
+                }
+            }
+            add_count(a.count, c);
+            return;
+        }
+    }
     for (uint64_t i = gid; i < a.n; i += ngroups) {
+        if constexpr (OP == OP_INSERT) {
+            if (a.region_cap) {
+                // past the keys of this region's run: nothing there
+                const uint64_t r = __umul64hi(a.region_div, i);
+                if (i - r * a.region_cap >= a.region_cursor[r] - r * a.region_cap) continue;
+            }
+        }
         const uint64_t key = __ldg(a.keys + i);
         bool r;
         if constexpr (OP == OP_INSERT) {

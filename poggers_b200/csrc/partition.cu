@@ -16,6 +16,7 @@
 // visits the keys changes, and concurrent inserts have no defined order in
 // the reference either.  The caller's ok flags are preset to 1 and a failed
 // insert clears its flag through the permutation.
+#include <math.h>
 #include <stdint.h>
 #include <cuda_runtime.h>
 
@@ -100,14 +101,23 @@ __global__ void k_part_scan(const unsigned long long *counts, unsigned long long
     }
 }
 
+// cursors[r] = r * cap: the start of region r's run of cap entries
+__global__ void k_part_bases(unsigned long long *cursors, uint32_t R, uint64_t cap)
+{
+    for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) cursors[r] = (unsigned long long)r * cap;
+}
+
 // One tile of kPartTile keys at a time: count the tile's keys per region in
 // shared memory, reserve one run per region from the global cursors, sort the
 // tile by region in shared memory, then write each region's run with
-// consecutive threads on consecutive addresses.
+// consecutive threads on consecutive addresses.  With cap != 0 region r owns
+// the cap entries from r * cap; a key reserved past them is not written and
+// its bit (by its index in the batch) is set in ovf instead.
 template <class Router, class V>
 __global__ void __launch_bounds__(kPartThreads) k_part_scatter(Router route, const uint64_t *keys, const V *vals,
                                                                uint64_t n, uint32_t R, unsigned long long *cursors,
-                                                               uint64_t *okeys, V *ovals, uint32_t *operm)
+                                                               uint64_t *okeys, V *ovals, uint32_t *operm,
+                                                               uint64_t cap, uint32_t *ovf)
 {
     __shared__ unsigned long long gbase[kPartMaxRegions];
     __shared__ unsigned int cnt[kPartMaxRegions];
@@ -175,6 +185,10 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(Router route, con
         for (uint32_t e = tid; e < tn; e += blockDim.x) {
             const uint32_t r = sr[e];
             const uint64_t pos = gbase[r] + (e - lstart[r]);
+            if (cap && pos >= (uint64_t)(r + 1) * cap) {
+                atomicOr(ovf + (sp[e] >> 5), 1u << (sp[e] & 31u));
+                continue;
+            }
             okeys[pos] = sk[e];
             if (ovals) ovals[pos] = sv[e];
             operm[pos] = sp[e];
@@ -189,19 +203,24 @@ using namespace pg;
 
 // Called by pg_bulk_insert with the caller's batch in `a`.  When the batch
 // qualifies it writes the region-ordered copy into the table's scratch,
-// presets the ok flags to 1, points `a` at the copy and returns true; the
-// caller then runs the ordinary insert launch on `a`.  Returns false (and
-// leaves `a` alone) when the batch should take the ordinary path: partitioning
-// off, a serial launch shape, not a uint64 bucket table, table or batch too
-// small for the sort to pay, or no memory for the scratch.
+// presets the ok flags to 1, points `a` at the copy (in runs, one per region)
+// and returns true; the caller then runs the ordinary insert launch on `a`,
+// and after it the keys that did not fit their run, from the caller's batch
+// (bits in a.only, returned through `only`).  Returns false (and leaves `a`
+// alone) when the batch should take the ordinary path: partitioning off, a
+// serial launch shape, not a uint64 bucket table, table or batch too small
+// for the sort to pay, or no memory for the scratch.
+//
+// The runs have a fixed capacity: the keys expected in a full region (the
+// first bucket is MurmurHash64A % nb, uniform over the buckets) plus eight
+// standard deviations and 1024, so the sort needs no counting pass.  Only a
+// batch far from uniform over the table (many copies of one key, say) fills
+// a run; its extra keys are inserted by the second pass, in batch order.
 namespace {
 
-// The region sort: sorts (keys, 8-byte values) into the table's scratch,
-// presets the flags to 1, and returns the sorted copy and the permutation;
-// false when the batch should run in batch order.
-bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&vals, uint8_t *flags,
-                 const uint32_t *&perm, cudaStream_t s)
+bool region_sort(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t s)
 {
+    const uint64_t n = a.n;
     if (t->bytes[0] < 2 * kPartRegionBytes || n < kPartMinKeys || n >= (1ull << 32)) return false;
     // regions of 2^shift buckets, about kPartRegionBytes of slots each, at most kPartMaxRegions
     const uint64_t nb = t->desc.lv[0].nbmod.d, bucket_bytes = t->bytes[0] / nb;
@@ -209,9 +228,15 @@ bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&va
     while ((bucket_bytes << (shift + 1)) <= kPartRegionBytes) shift++;
     while (((nb - 1) >> shift) + 1 > kPartMaxRegions) shift++;
     const uint32_t R = (uint32_t)(((nb - 1) >> shift) + 1);
-    // scratch: keys (8 B), values (8 B), original index (4 B) per key; counts and cursors per region
-    const uint64_t cnt_off = (n * 20 + 255) & ~255ull;
-    const uint64_t need = cnt_off + 2ull * R * 8;
+    const double expect = (double)n * (double)(1ull << shift) / (double)nb;
+    const uint64_t cap = (uint64_t)(expect + 8.0 * sqrt(expect)) + 1024;
+    const uint64_t nv = cap * R;  // entries of the sorted copy, runs included
+    if (nv >= (1ull << 32)) return false;
+    // scratch: keys (8 B), values (8 B) and original index (4 B) per entry;
+    // run cursors; one overflow bit per key of the batch
+    const uint64_t cur_off = (nv * 20 + 255) & ~255ull;
+    const uint64_t ovf_off = cur_off + ((R * 8ull + 255) & ~255ull);
+    const uint64_t need = ovf_off + ((n + 31) / 32) * 4;
     if (t->part_bytes < need) {
         if (t->part_buf) cudaFree(t->part_buf);
         t->part_buf = nullptr;
@@ -224,32 +249,36 @@ bool region_sort(pg_table *t, uint64_t n, const uint64_t *&keys, const void *&va
     }
     unsigned char *p = static_cast<unsigned char *>(t->part_buf);
     uint64_t *okeys = reinterpret_cast<uint64_t *>(p);
-    void *ovals = vals ? static_cast<void *>(p + n * 8) : nullptr;
-    uint32_t *operm = reinterpret_cast<uint32_t *>(p + n * 16);
-    unsigned long long *counts = reinterpret_cast<unsigned long long *>(p + cnt_off);
-    unsigned long long *cursors = counts + R;
-    const level_desc &L = t->desc.lv[0];
+    void *ovals = a.vals_in ? static_cast<void *>(p + nv * 8) : nullptr;
+    uint32_t *operm = reinterpret_cast<uint32_t *>(p + nv * 16);
+    unsigned long long *cursors = reinterpret_cast<unsigned long long *>(p + cur_off);
+    uint32_t *ovf = reinterpret_cast<uint32_t *>(p + ovf_off);
     const unsigned grid = (unsigned)(t->num_sms * 8);
-    cudaMemsetAsync(counts, 0, R * 8, s);
-    const region_router route{L, shift};
-    k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, R, counts);
-    k_part_scan<<<1, 32, 0, s>>>(counts, cursors, R);
-    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const unsigned long long *>(vals), n, R,
-                                                 cursors, okeys, static_cast<unsigned long long *>(ovals), operm);
-    if (flags) cudaMemsetAsync(flags, 1, n, s);
-    keys = okeys;
-    vals = ovals;
-    perm = operm;
+    cudaMemsetAsync(ovf, 0, ((n + 31) / 32) * 4, s);
+    k_part_bases<<<1, kPartThreads, 0, s>>>(cursors, R, cap);
+    const region_router route{t->desc.lv[0], shift};
+    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
+                                                 R, cursors, okeys, static_cast<unsigned long long *>(ovals), operm,
+                                                 cap, ovf);
+    if (a.flags) cudaMemsetAsync(a.flags, 1, n, s);
+    a.keys = okeys;
+    a.vals_in = ovals;
+    a.perm = operm;
+    a.n = nv;
+    a.region_cursor = cursors;
+    a.region_cap = cap;
+    a.region_div = ~0ull / cap + 1;
+    only = ovf;
     return true;
 }
 
 }  // namespace
 
-bool pg_partition_insert(pg_table *t, bulk_args &a, cudaStream_t s)
+bool pg_partition_insert(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t s)
 {
     const bool kv64 = t->ifmt == FMT_KV64 || t->ifmt == FMT_KV64_SPLIT || t->ifmt == FMT_KV64_FP;
     if (!t->partition || !kv64 || t->cfg.levels[0].scheme != PG_SCHEME_BUCKET || t->max_blocks == 1) return false;
-    return region_sort(t, a.n, a.keys, a.vals_in, a.flags, a.perm, s);
+    return region_sort(t, a, only, s);
 }
 
 // ---------------------------------------------------------------- sharding
@@ -278,7 +307,7 @@ pg_status route_t(const uint64_t *keys, const void *vals, uint64_t n, uint32_t n
     k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, nshards, c);
     k_part_scan<<<1, 32, 0, s>>>(c, cur, nshards);
     k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const V *>(vals), n, nshards, cur, okeys,
-                                                 static_cast<V *>(ovals), operm);
+                                                 static_cast<V *>(ovals), operm, 0, nullptr);
     return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
 }
 

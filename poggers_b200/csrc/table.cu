@@ -399,7 +399,16 @@ pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals
     }
     bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
                 reinterpret_cast<unsigned long long *>(d_fail_count), n};
-    if (t && d_keys && n) pg_partition_insert(t, a, reinterpret_cast<cudaStream_t>(stream));
+    const bulk_args batch = a;
+    const uint32_t *only = nullptr;
+    if (t && d_keys && n && pg_partition_insert(t, a, only, reinterpret_cast<cudaStream_t>(stream))) {
+        // the sorted runs, then any keys that did not fit their run
+        const pg_status st = run_bulk(t, OP_INSERT, a, stream);
+        if (st != PG_OK) return st;
+        bulk_args rest = batch;
+        rest.only = only;
+        return run_bulk(t, OP_INSERT, rest, stream);
+    }
     return run_bulk(t, OP_INSERT, a, stream);
 }
 

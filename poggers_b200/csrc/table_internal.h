@@ -28,5 +28,6 @@ struct pg_table {
 uint32_t pg_table_lanes(const pg_table *t, int op = 1);
 
 namespace pg { struct bulk_args; }
-// Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted copy.
-bool pg_partition_insert(pg_table *t, pg::bulk_args &a, cudaStream_t s);
+// Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted
+// copy; `only` then marks the keys of the caller's batch left for a second pass.
+bool pg_partition_insert(pg_table *t, pg::bulk_args &a, const uint32_t *&only, cudaStream_t s);

@@ -123,3 +123,31 @@ def test_bucketed_filter_keeps_batch_order(pg, bits):
         backing.append(t.get_fill(1)[0])
         t.free_on_device()
     assert abs(backing[0] - backing[1]) <= max(500, backing[1] // 10), backing
+
+
+def test_ordered_insert_with_a_full_run(pg):
+    """A batch far from uniform over the table: 2^19 copies of one key on top of
+    2^21 distinct keys.  The copies overflow their region's run; those that do
+    not fit are inserted by the second pass in batch order.  Both runs (sorted
+    and batch order) place every distinct key, place the same number of copies
+    (at most 20 probes x 8 slots), and report each failure at its own batch
+    position."""
+    uniq = wl.keys_without_sentinels(15, 1 << 21)
+    dup = np.full(1 << 19, uniq[0], dtype=np.uint64)
+    keys = np.concatenate([uniq[: 1 << 20], dup, uniq[1 << 20:]])
+    vals = wl.values_for(keys, 8, 16)
+    is_dup = np.zeros(len(keys), dtype=bool)
+    is_dup[1 << 20: (1 << 20) + (1 << 19)] = True
+    is_dup[0] = True  # the first copy of the key is uniq[0] itself
+    placed = []
+    for part in (True, False):
+        t = _table(pg, "fingerprints", part)
+        d = Driver(t)
+        ok = d.insert(keys, vals)
+        assert ok[~is_dup].all()
+        f, v = d.query(uniq)
+        assert f.all() and (v[1:] == vals[~is_dup]).all()
+        placed.append(int(ok[is_dup].sum()))
+        assert t.get_fill(0)[0] == int(ok.sum())
+        t.free_on_device()
+    assert placed[0] <= 160 and abs(placed[0] - placed[1]) <= 8, placed
