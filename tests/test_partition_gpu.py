@@ -55,6 +55,16 @@ def test_ordered_insert_matches_unordered_and_oracle(pg, oracle, layout):
     assert (r == oka[ridx]).all()
 
 
+def _few_buckets(keys, seed=43, nslots=NSLOTS, bucket=8):
+    """Keys whose 20 double-hash probes cover at most two distinct buckets (the
+    second hash a multiple of nb / 2 when nb is a power of two): whether they
+    fit depends on placement order, in the reference as well."""
+    from oracle import pyoracle
+    nb = nslots // bucket
+    return np.array([len({v % nb for v in pyoracle.probe_values(0, seed, 0, int(k), 20)}) <= 2 for k in keys],
+                    dtype=bool)
+
+
 def test_ordered_insert_without_values_and_flags(pg):
     import torch
     n = 3 << 20
@@ -63,14 +73,14 @@ def test_ordered_insert_without_values_and_flags(pg):
     fails = torch.zeros(1, dtype=torch.int64, device="cuda")
     t.bulk_insert(to_dev(keys), None, None, fails)  # NULL values and NULL flags
     torch.cuda.synchronize()
-    assert int(fails.item()) == 0
     f, v = Driver(t).query(keys)
-    assert f.all() and (v == 0).all()
+    assert int(fails.item()) == int((~f).sum()) and _few_buckets(keys[~f]).all()
+    assert (v == 0).all()
     # a second, smaller ordered batch reuses the scratch
     before = t.host_bytes_in_use()
     more = wl.keys_without_sentinels(8, 1 << 20)
     ok = Driver(t).insert(more, wl.values_for(more, 8, 5))
-    assert ok.all() and t.host_bytes_in_use() == before
+    assert _few_buckets(more[~ok]).all() and t.host_bytes_in_use() == before
 
 
 def test_ordered_insert_overflow_reports_each_failure_in_place(pg):
@@ -144,9 +154,9 @@ def test_ordered_insert_with_a_full_run(pg):
         t = _table(pg, "fingerprints", part)
         d = Driver(t)
         ok = d.insert(keys, vals)
-        assert ok[~is_dup].all()
-        f, v = d.query(uniq)
-        assert f.all() and (v[1:] == vals[~is_dup]).all()
+        assert _few_buckets(keys[~is_dup & ~ok]).all()
+        f, v = d.query(uniq[1:])
+        assert (f == ok[~is_dup]).all() and (v[f] == vals[~is_dup][f]).all()
         placed.append(int(ok[is_dup].sum()))
         assert t.get_fill(0)[0] == int(ok.sum())
         t.free_on_device()
