@@ -113,15 +113,22 @@ __global__ void k_part_bases(unsigned long long *cursors, uint32_t R, uint64_t c
 // consecutive threads on consecutive addresses.  With cap != 0 region r owns
 // the cap entries from r * cap; a key reserved past them is not written and
 // its bit (by its index in the batch) is set in ovf instead.
+// The per-region arrays take part_scatter_smem(R) bytes of dynamic shared
+// memory (22.5 KB per block in all at 32 regions instead of 38.9 KB sized for
+// the most regions; more resident blocks, forced by register limits of 40 or
+// 32, measured 2 % slower).
+inline size_t part_scatter_smem(uint32_t R) { return (size_t)R * (sizeof(unsigned long long) + 2 * sizeof(unsigned)); }
+
 template <class Router, class V>
-__global__ void __launch_bounds__(kPartThreads) k_part_scatter(Router route, const uint64_t *keys, const V *vals,
-                                                               uint64_t n, uint32_t R, unsigned long long *cursors,
-                                                               uint64_t *okeys, V *ovals, uint32_t *operm,
-                                                               uint64_t cap, uint32_t *ovf)
+__global__ void __launch_bounds__(kPartThreads)
+    k_part_scatter(Router route, const uint64_t *keys, const V *vals, uint64_t n, uint32_t R,
+                   unsigned long long *cursors, uint64_t *okeys, V *ovals, uint32_t *operm, uint64_t cap,
+                   uint32_t *ovf)
 {
-    __shared__ unsigned long long gbase[kPartMaxRegions];
-    __shared__ unsigned int cnt[kPartMaxRegions];
-    __shared__ unsigned int lstart[kPartMaxRegions];
+    extern __shared__ unsigned long long part_dyn[];
+    unsigned long long *gbase = part_dyn;                                 // R reservations
+    unsigned int *cnt = reinterpret_cast<unsigned int *>(gbase + R);      // R tile counts
+    unsigned int *lstart = cnt + R;                                       // R tile offsets
     __shared__ uint64_t sk[kPartTile];
     __shared__ V sv[kPartTile];
     __shared__ uint32_t sp[kPartTile];
@@ -257,9 +264,9 @@ bool region_sort(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t 
     cudaMemsetAsync(ovf, 0, ((n + 31) / 32) * 4, s);
     k_part_bases<<<1, kPartThreads, 0, s>>>(cursors, R, cap);
     const region_router route{t->desc.lv[0], shift};
-    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, a.keys, static_cast<const unsigned long long *>(a.vals_in), n,
-                                                 R, cursors, okeys, static_cast<unsigned long long *>(ovals), operm,
-                                                 cap, ovf);
+    k_part_scatter<<<grid, kPartThreads, part_scatter_smem(R), s>>>(
+        route, a.keys, static_cast<const unsigned long long *>(a.vals_in), n, R, cursors, okeys,
+        static_cast<unsigned long long *>(ovals), operm, cap, ovf);
     if (a.flags) cudaMemsetAsync(a.flags, 1, n, s);
     a.keys = okeys;
     a.vals_in = ovals;
@@ -306,8 +313,8 @@ pg_status route_t(const uint64_t *keys, const void *vals, uint64_t n, uint32_t n
     if (cudaMemsetAsync(c, 0, nshards * sizeof(unsigned long long), s) != cudaSuccess) return PG_ERR_CUDA;
     k_part_count<<<grid, kPartThreads, 0, s>>>(route, keys, n, nshards, c);
     k_part_scan<<<1, 32, 0, s>>>(c, cur, nshards);
-    k_part_scatter<<<grid, kPartThreads, 0, s>>>(route, keys, static_cast<const V *>(vals), n, nshards, cur, okeys,
-                                                 static_cast<V *>(ovals), operm, 0, nullptr);
+    k_part_scatter<<<grid, kPartThreads, part_scatter_smem(nshards), s>>>(
+        route, keys, static_cast<const V *>(vals), n, nshards, cur, okeys, static_cast<V *>(ovals), operm, 0, nullptr);
     return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
 }
 
