@@ -290,15 +290,12 @@ def config4(args):
 
 
 # ---------------------------------------------------------------- delete flow
-def config_del(args):
-    """The reference's delete test (tests/src/delete_tests.cu:568-760) on the
-    bucketed filter with tombstone reuse: 2^log2 primary slots + 1% backing,
-    16-bit tags; insert 0.9 of the slots, remove the first half, query the
-    second half, re-add the first half with insert_with_delete.  Each phase is
-    timed with CUDA events, for this library and (when its build is present)
-    for the reference's own CUDA build on the same GPU, same keys."""
+def del_flow(log2):
+    """Inputs of the reference's delete test (tests/src/delete_tests.cu:568-760)
+    at 2^log2 primary slots + 1 % backing: 0.9 of the slots in seeded keys and
+    16-bit values, on the device, with the halves the phases use."""
     import torch
-    n0 = 1 << args.log2
+    n0 = 1 << log2
     n1 = n0 // 100
     n = int(0.9 * (n0 + n1))
     half = n // 2
@@ -306,38 +303,54 @@ def config_del(args):
     vals = (wl.values_for(keys, 2, 49).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
     dk = torch.from_numpy(keys.view(np.int64)).cuda()
     dv = torch.from_numpy(vals.view(np.int16)).cuda()
-    dk1, dk2, dv1 = dk[:half].contiguous(), dk[half:].contiguous(), dv[:half].contiguous()
-    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
-    qv = torch.zeros(n - half, dtype=torch.int16, device="cuda")
+    return {"n0": n0, "n1": n1, "n": n, "half": half, "dk": dk, "dv": dv, "dk1": dk[:half].contiguous(),
+            "dk2": dk[half:].contiguous(), "dv1": dv[:half].contiguous(),
+            "ok": torch.zeros(n, dtype=torch.uint8, device="cuda"),
+            "qv": torch.zeros(n - half, dtype=torch.int16, device="cuda")}
 
-    def phases(run):
-        e = _events(5)
-        e[0].record()
-        run(0, dk, dv, ok)
-        e[1].record()
-        run(2, dk1, None, ok[:half])
-        e[2].record()
-        run(1, dk2, None, ok[half:], qv)
-        e[3].record()
-        run(3, dk1, dv1, ok[:half])
-        e[4].record()
-        torch.cuda.synchronize()
-        return [e[i].elapsed_time(e[i + 1]) for i in range(4)]
 
-    def summarize(ms):
-        med = np.median(np.array(ms), axis=0)
-        units = [n, half, n - half, half]
-        names = ["insert", "remove", "query", "insert_with_delete"]
-        out = {f"{k}_mops": round(u / m / 1e3, 1) for k, u, m in zip(names, units, med)}
-        out["total_mops"] = round(sum(units) / med.sum() / 1e3, 1)
-        out["ms"] = [round(float(x), 3) for x in med]
-        return out
+def del_phases(run, d):
+    """Insert all, remove the first half, query the second half, re-add the first
+    half with insert_with_delete; run(op, keys, vals, flags[, vals_out]) with
+    op 0 insert, 1 query, 2 remove, 3 insert_with_delete.  CUDA-event ms per phase."""
+    import torch
+    half, ok = d["half"], d["ok"]
+    e = _events(5)
+    e[0].record()
+    run(0, d["dk"], d["dv"], ok)
+    e[1].record()
+    run(2, d["dk1"], None, ok[:half])
+    e[2].record()
+    run(1, d["dk2"], None, ok[half:], d["qv"])
+    e[3].record()
+    run(3, d["dk1"], d["dv1"], ok[:half])
+    e[4].record()
+    torch.cuda.synchronize()
+    return [e[i].elapsed_time(e[i + 1]) for i in range(4)]
 
+
+def del_summary(ms, d):
+    med = np.median(np.array(ms), axis=0)
+    n, half = d["n"], d["half"]
+    units = [n, half, n - half, half]
+    names = ["insert", "remove", "query", "insert_with_delete"]
+    out = {f"{k}_mops": round(u / m / 1e3, 1) for k, u, m in zip(names, units, med)}
+    out["total_mops"] = round(sum(units) / med.sum() / 1e3, 1)
+    out["ms"] = [round(float(x), 3) for x in med]
+    return out
+
+
+def config_del(args):
+    """The reference's delete test on the bucketed filter with tombstone reuse:
+    2^log2 primary slots + 1 % backing, 16-bit tags.  Each phase is timed with
+    CUDA events, at 1 and 4 lanes per key.  (oracle/time_refcuda.py times the
+    reference's own CUDA build on the same keys.)"""
+    d = del_flow(args.log2)
     res = {"config": "del", "workload": f"bucketed filter, 16-bit tags: 2^{args.log2} slots (16/bucket) + 1% "
                                        f"backing (8/bucket, linear), 0.9 load; insert, remove 1/2, query 1/2, "
-                                       f"re-add 1/2", "keys": n}
+                                       f"re-add 1/2", "keys": d["n"]}
     for lanes in (1, 4):
-        t = pg.Table(pg.data_structs.del_tcf(n0, n1), 42)
+        t = pg.Table(pg.data_structs.del_tcf(d["n0"], d["n1"]), 42)
         t.set_launch(256, 32, 0, lanes)
 
         def run(op, k, v, fl, out=None):
@@ -353,32 +366,98 @@ def config_del(args):
         ms = []
         for step in range(args.steps + 2):
             t.clear()
-            m = phases(run)
+            m = del_phases(run, d)
             if step >= 2:
                 ms.append(m)
-        res[f"ours_lanes{lanes}"] = summarize(ms)
+        res[f"ours_lanes{lanes}"] = del_summary(ms, d)
         del t
-    try:
-        from oracle import pyrefcuda as rc
-        if rc.available():
-            ms = []
-            for step in range(args.steps + 2):
-                r = rc.RefTable(rc.KIND_DEL_TCF, n0, n1, 42)
-
-                def rrun(op, k, v, fl, out=None):
-                    r.bbulk(op if op != 3 else rc.OP_INSERT_DELETE, k, v, fl, out)
-
-                m = phases(rrun)
-                r.close()
-                if step >= 2:
-                    ms.append(m)
-            res["reference_cuda"] = summarize(ms)
-    except (ImportError, RuntimeError) as e:
-        res["reference_cuda"] = f"unavailable: {e}"
     return res
 
 
-# ---------------------------------------------------------------- config 5
+# ---------------------------------------------------------------- config tcf
+# The two-choice filters of the reference's data_structs (tcf.cuh:30, with a
+# 1 % backing table; and the tag-only filter of bucket_speed_tests.cu:108)
+# at an L2-resident and an HBM-resident size.
+TCF_WORKLOADS = [
+    # name, log2 slots, backing fraction, load, values
+    ("tcf_2p22", 22, 100, 0.85, True),
+    ("tcf_2p28", 28, 100, 0.85, True),
+    ("tag_only_2p28", 28, 0, 0.9, False),
+]
+
+
+def tcf_inputs(log2, load, values):
+    import torch
+    n = int(load * (1 << log2))
+    keys = wl.keys_without_sentinels(42, n)
+    fresh = wl.keys_without_sentinels(4242, n)
+    vals = (wl.values_for(keys, 2, 49).astype(np.uint64) & np.uint64(0xFFFF)).astype(np.uint16)
+    return {"n": n, "dk": torch.from_numpy(keys.view(np.int64)).cuda(),
+            "df": torch.from_numpy(fresh.view(np.int64)).cuda(),
+            "dv": torch.from_numpy(vals.view(np.int16)).cuda() if values else None,
+            "ok": torch.zeros(n, dtype=torch.uint8, device="cuda"),
+            "found": torch.zeros(n, dtype=torch.uint8, device="cuda")}
+
+
+def tcf_phases(run, d):
+    """Insert all keys, query them, query as many absent keys; run(op, keys,
+    vals, flags) with op 0 insert, 1 query.  Returns CUDA-event ms per phase and
+    the failures, false negatives and false positives of the run."""
+    import torch
+    e = _events(4)
+    e[0].record()
+    run(0, d["dk"], d["dv"], d["ok"])
+    e[1].record()
+    run(1, d["dk"], None, d["found"])
+    e[2].record()
+    fn = int(((d["found"] == 0) & (d["ok"] == 1)).sum().item())
+    e2 = _events(2)
+    e2[0].record()
+    run(1, d["df"], None, d["found"])
+    e2[1].record()
+    torch.cuda.synchronize()
+    return ([e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), e2[0].elapsed_time(e2[1])],
+            int((d["ok"] == 0).sum().item()), fn, int(d["found"].sum().item()))
+
+
+def tcf_summary(runs, d):
+    ms = np.median(np.array([r[0] for r in runs]), axis=0)
+    n = d["n"]
+    return {"insert_mops": round(n / ms[0] / 1e3, 1), "query_positive_mops": round(n / ms[1] / 1e3, 1),
+            "query_negative_mops": round(n / ms[2] / 1e3, 1),
+            "insert_query_mops": round(3 * n / ms.sum() / 1e3, 1), "ms": [round(float(x), 3) for x in ms],
+            "insert_failures": runs[-1][1], "false_negatives": runs[-1][2], "fp_rate": runs[-1][3] / n}
+
+
+def config_tcf(args):
+    """The TCF and the tag-only filter: insert to their load, query the keys,
+    query as many absent keys (default launch shape).  (oracle/time_refcuda.py
+    times the reference's own CUDA build on the same keys.)"""
+    res = {"config": "tcf", "workload": "TCF (16-bit tags + values, 16-slot buckets, 1 % backing) at 0.85 load "
+                                        "and the tag-only filter at 0.9 load; insert, query inserted, query absent"}
+    for name, log2, backing, load, values in TCF_WORKLOADS:
+        d = tcf_inputs(log2, load, values)
+        n0 = 1 << log2
+        cfg = pg.data_structs.tcf(n0, n0 // backing) if backing else pg.data_structs.tcqf(n0)
+        t = pg.Table(cfg, 42)
+
+        def run(op, k, v, fl):
+            if op == 0:
+                t.bulk_insert(k, v, fl)
+            else:
+                t.bulk_query(k, None, fl)
+
+        runs = []
+        for step in range(args.steps + 2):
+            t.clear()
+            r = tcf_phases(run, d)
+            if step >= 2:
+                runs.append(r)
+        res[name] = tcf_summary(runs, d)
+        del t, d
+    return res
+
+
 def _timed(fn):
     import torch
     e = _events(2)
@@ -564,7 +643,7 @@ def srv_config_of(kind, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["1", "3", "4", "5", "del"], required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf"], required=True)
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--tables", type=int, default=1024)
@@ -578,7 +657,7 @@ def main():
     a = ap.parse_args()
     import torch
     torch.cuda.init()
-    fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del}[a.config]
+    fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del, "tcf": config_tcf}[a.config]
     print(json.dumps(fn(a)))
 
 
