@@ -3,10 +3,14 @@
     python -m poggers_b200.bench_configs --config 1   # plain TCF, 2^22 slots
     python -m poggers_b200.bench_configs --config 3   # 1024 TCFs: batched vs per-table launches
     python -m poggers_b200.bench_configs --config 4   # served request stream vs plain per-request path
-    python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots), ours vs reference
+    python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots)
+    python -m poggers_b200.bench_configs --config tcf # TCF and tag-only filter, 2^22 and 2^28 slots
     python -m poggers_b200.bench_configs --config 5   # large: 2^30-slot HT, 2^32-slot tag-only TCF, slab churn, served HT
 
-Each prints one JSON line.  All inputs are seeded synthetic keys.
+Each prints one JSON line.  All inputs are seeded synthetic keys.  The
+reference's own CUDA build is timed on the same keys by oracle/time_refcuda.py
+(configs del and tcf).  hbm_frac fields are algorithmic bytes per operation x
+operations per second over the measured HBM copy bandwidth.
 """
 from __future__ import annotations
 
@@ -18,6 +22,23 @@ import numpy as np
 
 import poggers_b200 as pg
 from poggers_b200 import workload as wl
+
+
+# algorithmic bytes per operation: one minimal pass over each touched bucket
+# (TCF: 8 B key + two 32 B buckets (+ a 32 B sector written); uint64 table:
+# key and value + a 128 B bucket (+ a 32 B sector written); slab: an 8 B
+# pointer + a 32 B bitmap sector)
+ALGO_BYTES = {"tcf_insert": 104, "tcf_query": 73, "ht_insert": 176, "ht_query": 145, "slab": 40}
+
+
+def hbm_frac(bytes_per_op, mops):
+    """bytes_per_op x mops (millions of operations per second) over the measured
+    HBM copy bandwidth (MEASURED_PEAKS.json at the repository root; 6650 GB/s
+    when it is absent)."""
+    from pathlib import Path
+    p = Path(__file__).resolve().parent.parent / "MEASURED_PEAKS.json"
+    peak = float(json.loads(p.read_text())["hbm_gbs"]) if p.exists() else 6650.0
+    return round(bytes_per_op * mops * 1e6 / (peak * 1e9), 3)
 
 
 def _dev(a):
@@ -423,10 +444,14 @@ def tcf_phases(run, d):
 def tcf_summary(runs, d):
     ms = np.median(np.array([r[0] for r in runs]), axis=0)
     n = d["n"]
-    return {"insert_mops": round(n / ms[0] / 1e3, 1), "query_positive_mops": round(n / ms[1] / 1e3, 1),
-            "query_negative_mops": round(n / ms[2] / 1e3, 1),
+    mops = [n / m / 1e3 for m in ms]
+    return {"insert_mops": round(mops[0], 1), "query_positive_mops": round(mops[1], 1),
+            "query_negative_mops": round(mops[2], 1),
             "insert_query_mops": round(3 * n / ms.sum() / 1e3, 1), "ms": [round(float(x), 3) for x in ms],
-            "insert_failures": runs[-1][1], "false_negatives": runs[-1][2], "fp_rate": runs[-1][3] / n}
+            "insert_failures": runs[-1][1], "false_negatives": runs[-1][2], "fp_rate": runs[-1][3] / n,
+            "hbm_frac": {"insert": hbm_frac(ALGO_BYTES["tcf_insert"], mops[0]),
+                         "query_positive": hbm_frac(ALGO_BYTES["tcf_query"], mops[1]),
+                         "query_negative": hbm_frac(ALGO_BYTES["tcf_query"], mops[2])}}
 
 
 def config_tcf(args):
@@ -630,6 +655,12 @@ def config5(args):
                              "query_p50_ms": round(1e3 * float(np.percentile(lat_q, 50)), 2),
                              "query_p99_ms": round(1e3 * float(np.percentile(lat_q, 99)), 2),
                              "note": "host numpy buffers in, values out; per wave: host copies into pinned staging (split over threads), PCIe transfers and kernels, two waves in flight"}
+    ht, tcf, slab = res["ht_2p30"], res["tcf_2p32_tag_only"], res["slab_churn"]
+    ht["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["ht_insert"], ht["insert_mops"]),
+                      "query": hbm_frac(ALGO_BYTES["ht_query"], ht["query_mops"])}
+    tcf["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["tcf_insert"], tcf["insert_mops"]),
+                       "query": hbm_frac(ALGO_BYTES["tcf_query"], tcf["query_mops"])}
+    slab["hbm_frac"] = {k: hbm_frac(ALGO_BYTES["slab"], slab[k + "_mops"]) for k in ("malloc", "free", "remalloc")}
     return res
 
 
