@@ -6,6 +6,7 @@
     python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots)
     python -m poggers_b200.bench_configs --config tcf # TCF and tag-only filter, 2^22 and 2^28 slots
     python -m poggers_b200.bench_configs --config 5   # large: 2^30-slot HT, 2^32-slot tag-only TCF, slab churn, served HT
+    python -m poggers_b200.bench_configs --config gather  # the HBM ceiling for random 32- and 8-byte reads
 
 Each prints one JSON line.  All inputs are seeded synthetic keys.  The
 reference's own CUDA build is timed on the same keys by oracle/time_refcuda.py
@@ -672,9 +673,38 @@ def srv_config_of(kind, n):
     return pg.data_structs.tcf(int(n * 0.95), int(n * 0.05))
 
 
+def config_gather(args):
+    """The HBM ceiling for random accesses, the filters' regime: random 8-byte
+    words (each in its own 32-byte DRAM sector) gathered from a 4 GiB buffer by
+    torch's own index_select (library code, as the copy peak is torch's copy),
+    CUDA-event timed, best of 5 after one warm-up.  A filter's bucket is one or
+    two such sectors, so this rate, not the streaming copy bandwidth, bounds
+    the filters' kernels."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    buf = torch.randint(0, 1 << 62, (1 << 29,), dtype=torch.int64, device="cuda", generator=g)  # 4 GiB
+    n = 1 << 27
+    idx = torch.randint(0, buf.numel(), (n,), dtype=torch.int64, device="cuda", generator=g)
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    best = None
+    for _ in range(6):
+        e = _events(2)
+        e[0].record()
+        torch.index_select(buf, 0, idx, out=out)
+        e[1].record()
+        torch.cuda.synchronize()
+        ms = e[0].elapsed_time(e[1])
+        best = ms if best is None else min(best, ms)
+    g_per_s = n / best / 1e6
+    return {"config": "gather", "buffer_bytes": buf.numel() * 8, "reads": n, "ms": round(best, 3),
+            "random_sector_reads_g_per_s": round(g_per_s, 2), "sector_gbs": round(g_per_s * 32, 1),
+            "note": "each read also streams its 8-byte index and writes 8 bytes"}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf"], required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "gather"], required=True)
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--tables", type=int, default=1024)
@@ -688,7 +718,8 @@ def main():
     a = ap.parse_args()
     import torch
     torch.cuda.init()
-    fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del, "tcf": config_tcf}[a.config]
+    fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del, "tcf": config_tcf,
+          "gather": config_gather}[a.config]
     print(json.dumps(fn(a)))
 
 
