@@ -28,6 +28,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -210,9 +211,17 @@ void copy_all(const std::vector<copy_job> &jobs)
         part(0);
         return;
     }
+    // parts whose thread could not be started are copied here
     std::vector<std::thread> th;
-    for (unsigned k = 1; k < nt; k++) th.emplace_back(part, k);
-    part(0);
+    std::vector<unsigned> mine{0};
+    for (unsigned k = 1; k < nt; k++) {
+        try {
+            th.emplace_back(part, k);
+        } catch (const std::system_error &) {
+            mine.push_back(k);
+        }
+    }
+    for (unsigned k : mine) part(k);
     for (std::thread &t : th) t.join();
 }
 
