@@ -116,7 +116,9 @@ __global__ void k_part_bases(unsigned long long *cursors, uint32_t R, uint64_t c
 // The per-region arrays take part_scatter_smem(R) bytes of dynamic shared
 // memory (22.5 KB per block in all at 32 regions instead of 38.9 KB sized for
 // the most regions; more resident blocks, forced by register limits of 40 or
-// 32, measured 2 % slower).
+// 32, measured 2 % slower).  Tiles of 4 keys per thread: 2 measured 9 %
+// slower for the whole insert call, 8 the same (ncu: issue-bound with barrier
+// and shared-memory stalls at 45 % of DRAM peak, not bound by DRAM).
 inline size_t part_scatter_smem(uint32_t R) { return (size_t)R * (sizeof(unsigned long long) + 2 * sizeof(unsigned)); }
 
 template <class Router, class V>
