@@ -203,3 +203,39 @@ def test_bucketed_tags_and_tombstone_reuse(oracle):
     assert ok2.all() and o.level_bytes(0) != before
     f, v, found = o.bulk(oracle.BOP_INSERT_IF_NOT_EXISTS, new[:1], np.array([99], dtype=np.uint64))
     assert f[0] and found[0] and v[0] == 0
+
+
+@pytest.mark.parametrize("bits", [16, 8])
+def test_bucketed_oracle_sawtooth_keeps_its_fill(oracle, bits):
+    """The reference's sawtooth flow (tests/src/sawtooth_test.cu:624-826) on the
+    oracle: fill to 0.9 of a 2^14-slot filter with 2 % backing, then rounds of
+    removing half the live keys, querying the other half and re-adding fresh
+    keys with insert_with_delete.  After every round the live fill (both
+    levels) equals placed - removed + re-added, every queried key that was
+    placed and not removed by a same-tag neighbour is found, and re-adds reuse
+    the tombstones (the occupied count does not grow past the fill)."""
+    import poggers_b200 as pg
+    n0 = 1 << 14
+    cfg = pg.data_structs.del_tcf(n0, 2 * n0 // 100, tag_bits=bits)
+    levels = [(L.nslots, L.bucket_size, L.max_probes, L.scheme, L.probe) for L in cfg.levels]
+    o = oracle.OracleBucketed(bits, levels, 42)
+    mask = np.uint64((1 << bits) - 1)
+    n = int(0.9 * n0)
+    half = n // 2
+    live = wl.keys_without_sentinels(91, n)
+    vals = wl.values_for(live, 2, 92).astype(np.uint64) & mask
+    ok, _, _ = o.bulk(oracle.BOP_INSERT, live, vals)
+    placed = int(ok.sum())
+    occupied0 = o.count_fill(0) + o.count_fill(1)
+    assert occupied0 == placed
+    for rnd in range(3):
+        r, _, _ = o.bulk(oracle.BOP_REMOVE, live[:half])
+        f, _, _ = o.bulk(oracle.BOP_QUERY, live[half:])
+        fresh = wl.keys_without_sentinels(1000 + rnd, half)
+        fv = wl.values_for(fresh, 2, 2000 + rnd).astype(np.uint64) & mask
+        a, _, _ = o.bulk(oracle.BOP_INSERT_DELETE, fresh, fv)
+        placed += int(a.sum()) - int(r.sum())
+        assert o.count_fill(0) + o.count_fill(1) == placed, f"round {rnd}"
+        live[:half], vals[:half] = fresh, fv
+        # a query misses only where a remove took a same-tag slot of another key
+        assert (~f).sum() <= (20 if bits == 16 else 400), (rnd, int((~f).sum()))
