@@ -104,8 +104,10 @@ typedef struct pg_level_config {
 /* table flags */
 enum {
     /* Keep each bucket's keys contiguous, then its values ([B keys | B vals]),
-     * instead of the reference's {key, val} slots.  Same results; see the
-     * layout notes in DESIGN.md. */
+     * instead of the reference's {key, val} slots.  Same results, and dumps
+     * and images still use the reference's layout; a probe reads the keys
+     * without the values (for the TCF's 16-bit tags, one 32-byte sector per
+     * bucket). */
     PG_TABLE_SPLIT_BUCKETS = 1u,
     /* uint64 tables (PG_FMT_KV64, bucket_insert primary, reference layout):
      * keep one fingerprint byte per slot in a separate array (1/16 of the
