@@ -158,14 +158,39 @@ pg_status run_packed(pg_table *t, int op, const packed_args &a, pg_stream_t stre
     // one group per key, blocks in batch order like the reference's one-tile-per-key
     // launch: with deletes in the mix, which of two keys sharing a tag holds the
     // earlier slot (and so which one a remove takes) follows the batch order
-    dim3 grid, block;
     const uint32_t lanes = pg_table_lanes(t, op);
-    launch_shape(t, lanes, a.n, grid, block, true);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t b0 = t->cfg.levels[0].bucket_size, b1 = t->cfg.nlevels > 1 ? t->cfg.levels[1].bucket_size : 8;
-    const cudaError_t e = t->ifmt == FMT_PACKED16 ? launch_packed16(op, b0, b1, lanes, t->desc, a, grid, block, s)
-                                                  : launch_packed8(op, b0, b1, lanes, t->desc, a, grid, block, s);
-    return cuda_status(e);
+    // The insert forms into a two-choice primary level with fewer buckets than
+    // the GPU holds keys at once run in launches of one key per bucket: with the
+    // whole batch in flight together, every key's shortcut would see the fills
+    // from before the batch and keys would pile into their first choices (a
+    // 2^14-slot filter with 2 % backing filled to 0.9 failed ~340 keys in one
+    // launch; the sequential order fails none).  Larger levels are unaffected.
+    const bool inserts = op == POP_INSERT || op == POP_INSERT_DELETE || op == POP_INSERT_IF_NOT_EXISTS ||
+                         op == POP_INSERT_IF_NOT_EXISTS_DELETE;
+    const uint64_t nb0 = t->desc.lv[0].nbmod.d;
+    const uint64_t resident = (uint64_t)t->num_sms * 2048;
+    const uint64_t chunk = inserts && t->cfg.levels[0].scheme == PG_SCHEME_TWO_CHOICE_BUCKETED && nb0 < resident &&
+                                   t->max_blocks != 1
+                               ? nb0
+                               : a.n;
+    const uint32_t vb = t->ifmt == FMT_PACKED16 ? 2u : 1u;
+    for (uint64_t off = 0; off < a.n; off += chunk) {
+        packed_args c = a;
+        c.n = a.n - off < chunk ? a.n - off : chunk;
+        c.keys = a.keys + off;
+        if (a.vals_in) c.vals_in = static_cast<const unsigned char *>(a.vals_in) + off * vb;
+        if (a.vals_out) c.vals_out = static_cast<unsigned char *>(a.vals_out) + off * vb;
+        if (a.flags) c.flags = a.flags + off;
+        if (a.found) c.found = a.found + off;
+        dim3 grid, block;
+        launch_shape(t, lanes, c.n, grid, block, true);
+        const cudaError_t e = t->ifmt == FMT_PACKED16 ? launch_packed16(op, b0, b1, lanes, t->desc, c, grid, block, s)
+                                                      : launch_packed8(op, b0, b1, lanes, t->desc, c, grid, block, s);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return PG_OK;
 }
 
 // occupied / tombstone counts of one level: one thread per bucket
