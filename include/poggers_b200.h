@@ -314,7 +314,11 @@ pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_n
  * per call (larger calls return PG_ERR_TOO_LARGE).  That array (about 106 KB)
  * exists once on every GPU that loads the library, until the process exits.
  *  - The first call on a device looks up the array's device address; make that
- *    first call before capturing a stream into a CUDA graph.
+ *    first call before capturing a stream into a CUDA graph.  The address is
+ *    kept for the process's life, so do not use the call across a
+ *    cudaDeviceReset().
+ *  - The current device must be the tables' device (else PG_ERR_INVALID,
+ *    before anything is launched).
  *  - Every call shares the array and leaves its contents behind (the work
  *    counter is reset by each call), so calls whose work overlaps on the GPU
  *    (different streams, or different host threads) race: order them.
@@ -422,6 +426,27 @@ pg_slab *pg_slab_set_class(pg_slab_set *s, uint32_t c);
 pg_status pg_slab_set_bulk_malloc(pg_slab_set *s, const uint32_t *d_sizes, uint64_t n, void **d_ptrs,
                                   uint64_t *d_fail_count, pg_stream_t stream);
 pg_status pg_slab_set_bulk_free(pg_slab_set *s, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count,
+                                pg_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Diagnostics (no counterpart in the reference): the GPU's random-access
+ * ceilings, which bound the filters' kernels (one or two 32-byte sectors at
+ * random addresses per key, and an atomic claim on a sector just read).
+ * pg_diag_random_access makes about `accesses` accesses of one kind at
+ * hashed random offsets inside d_buf (64-byte aligned, >= 64 bytes), several
+ * in flight per thread, on blocks_per_sm (1-8, 0 = 8) blocks of 256 threads
+ * per SM; *accesses_done receives the exact count (rounded up to whole
+ * per-thread batches).  READ32: one 32-byte sector; READ64: two adjacent
+ * sectors; READ32_CAS: one sector, then a CAS on its first 4-byte word with
+ * the value read; RED32: an atomic add (no return) on a random 4-byte word.
+ * CAS and RED modes modify d_buf.  d_sink (8 bytes) only keeps the loads.
+ * --------------------------------------------------------------------------- */
+#define PG_DIAG_READ32 0
+#define PG_DIAG_READ64 1
+#define PG_DIAG_READ32_CAS 2
+#define PG_DIAG_RED32 3
+pg_status pg_diag_random_access(void *d_buf, uint64_t bytes, uint32_t mode, uint64_t accesses, uint64_t seed,
+                                uint32_t blocks_per_sm, uint64_t *accesses_done, uint64_t *d_sink,
                                 pg_stream_t stream);
 
 /* Host-side helpers used by tests (no GPU needed). */

@@ -29,6 +29,7 @@
 #pragma once
 #include <cooperative_groups.h>
 #include <stdexcept>
+#include <vector>
 #include <cstdint>
 #include <cstddef>
 #include "poggers_b200.h"
@@ -121,6 +122,29 @@ struct size_in_num_slots {
     {
         uint64_t t = 0;
         for (std::size_t j = 0; j < Num_Tables; j++) t += slots[j];
+        return t;
+    }
+};
+
+// variadic_size: one slot count per table level, as many as the constructor is
+// given (variadic_sizing.cuh:40-108), e.g. variadic_size(nslots, nslots / 100)
+// for a filter and its backing table.  The counts live in a vector, so the
+// object can be returned and copied by value; the cursor starts at the first
+// count.
+struct variadic_size {
+    std::vector<uint64_t> slots;
+    uint64_t i = 0;
+    template <class... T>
+    variadic_size(T... s) : slots{(uint64_t)s...}
+    {
+    }
+    uint64_t next() { return ++i <= slots.size() ? slots[i - 1] : end(); }
+    void reset() { i = 0; }
+    uint64_t end() const { return ~uint64_t(0); }
+    uint64_t total() const
+    {
+        uint64_t t = 0;
+        for (uint64_t s : slots) t += s;
         return t;
     }
 };
@@ -548,6 +572,24 @@ struct bucketed_table {
     __host__ static uint64_t get_block_size(uint64_t) { return 1024; }
     __host__ static uint64_t get_num_blocks(uint64_t n) { return (Partition_Size * n - 1) / get_block_size(n) + 1; }
     __host__ uint64_t host_bytes_in_use() { return pg_table_bytes(host_handle(this)); }
+    // bucketed_table::get_local_num_buckets / get_local_num_slots / get_num_slots
+    // (bucketed_table.cuh:444-486): buckets and slots of the primary level, and
+    // slots of every level
+    __host__ uint64_t get_local_num_buckets()
+    {
+        pg_level_info li{};
+        return pg_table_level_info(host_handle(this), 0, &li) == PG_OK ? li.nbuckets : 0;
+    }
+    __host__ uint64_t get_local_num_slots() { return get_local_num_buckets() * Bucket_Size; }
+    __host__ uint64_t get_num_slots()
+    {
+        uint64_t total = 0;
+        for (uint32_t l = 0; l < (Is_Recursive ? 2u : 1u); l++) {
+            pg_level_info li{};
+            if (pg_table_level_info(host_handle(this), l, &li) == PG_OK) total += li.nslots;
+        }
+        return total;
+    }
     // bucketed_table::get_fill (:498-548): live slots of every level
     __host__ uint64_t get_fill()
     {

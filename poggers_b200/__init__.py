@@ -33,6 +33,7 @@ LIB_PATH = Path(os.environ.get("POGGERS_B200_LIB", str(_PKG / "libpoggers_b200.s
 PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT, PG_ERR_TOO_LARGE = range(8)
 PG_STATIC_MAX_TABLES = 256
 PG_STATIC_MAX_OPS = 8192
+PG_DIAG_READ32, PG_DIAG_READ64, PG_DIAG_READ32_CAS, PG_DIAG_RED32 = 0, 1, 2, 3
 PG_TABLE_SPLIT_BUCKETS = 1
 PG_TABLE_FINGERPRINTS = 2
 FMT_KV64, FMT_TAGVAL16, FMT_TAG16, FMT_PACKED_TAGVAL16, FMT_PACKED_TAGVAL8 = 0, 1, 2, 3, 4
@@ -92,6 +93,7 @@ EXPORTED = (
     "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
+    "pg_diag_random_access",
 )
 PG_OP_INSERT, PG_OP_QUERY, PG_OP_REMOVE, PG_OP_INSERT_WITH_DELETE = 0, 1, 2, 3
 
@@ -211,6 +213,8 @@ def lib() -> C.CDLL:
     L.pg_host_fastmod.argtypes = [U64, U64]
     L.pg_host_probe_buckets.restype = U32
     L.pg_host_probe_buckets.argtypes = [C.POINTER(_TableConfig), U32, U64, U64, C.POINTER(U64), U32]
+    L.pg_diag_random_access.restype = C.c_int
+    L.pg_diag_random_access.argtypes = [P, U64, U32, U64, U64, U32, C.POINTER(U64), P, P]
     _lib = L
     return L
 
@@ -490,6 +494,20 @@ class data_structs:
     def two_choice_table_64(nslots: int, tile: int = 4, bucket: int = 8) -> TableConfig:
         # static_table<uint64,uint64,key_val_pair,4,B,power_of_n_insert_shortcut_scheme,2,powerOfTwoHasher>
         return TableConfig(FMT_KV64, tile, [Level(nslots, bucket, 2, SCHEME_TWO_CHOICE, PROBE_P2)])
+
+
+def diag_random_access(buf, mode: int, accesses: int, seed: int = 1, blocks_per_sm: int = 0, sink=None,
+                       stream=None) -> int:
+    """pg_diag_random_access over a device buffer (a CUDA tensor, 64-byte
+    aligned); returns the exact number of accesses launched."""
+    import torch
+    if sink is None:
+        sink = torch.zeros(1, dtype=torch.int64, device=buf.device)
+    done = C.c_uint64(0)
+    _check(lib().pg_diag_random_access(_ptr(buf), buf.numel() * buf.element_size(), mode, accesses, seed,
+                                       blocks_per_sm, C.byref(done), _ptr(sink), _stream(stream)),
+           "pg_diag_random_access")
+    return done.value
 
 
 def host_murmur64a(key: int, seed: int) -> int:

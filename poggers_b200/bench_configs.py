@@ -6,7 +6,7 @@
     python -m poggers_b200.bench_configs --config del # bucketed filter with deletes (2^28 slots)
     python -m poggers_b200.bench_configs --config tcf # TCF and tag-only filter, 2^22 and 2^28 slots
     python -m poggers_b200.bench_configs --config 5   # large: 2^30-slot HT, 2^32-slot tag-only TCF, slab churn, served HT
-    python -m poggers_b200.bench_configs --config gather  # the HBM ceiling for random 32- and 8-byte reads
+    python -m poggers_b200.bench_configs --config random  # the random-access ceilings (own kernel)
 
 Each prints one JSON line.  All inputs are seeded synthetic keys.  The
 reference's own CUDA build is timed on the same keys by oracle/time_refcuda.py
@@ -462,6 +462,11 @@ def config_tcf(args):
     res = {"config": "tcf", "workload": "TCF (16-bit tags + values, 16-slot buckets, 1 % backing) at 0.85 load "
                                         "and the tag-only filter at 0.9 load; insert, query inserted, query absent"}
     for name, log2, backing, load, values in TCF_WORKLOADS:
+        if args.only and name not in args.only:
+            continue
+        if args.tcf_log2:  # a smaller table of the same kind (profiling captures)
+            log2 = args.tcf_log2
+            name = f"{name}_at_2p{log2}"
         d = tcf_inputs(log2, load, values)
         n0 = 1 << log2
         cfg = pg.data_structs.tcf(n0, n0 // backing) if backing else pg.data_structs.tcqf(n0)
@@ -673,40 +678,53 @@ def srv_config_of(kind, n):
     return pg.data_structs.tcf(int(n * 0.95), int(n * 0.05))
 
 
-def config_gather(args):
-    """The HBM ceiling for random accesses, the filters' regime: random 8-byte
-    words (each in its own 32-byte DRAM sector) gathered from a 4 GiB buffer by
-    torch's own index_select (library code, as the copy peak is torch's copy),
-    CUDA-event timed, best of 5 after one warm-up.  A filter's bucket is one or
-    two such sectors, so this rate, not the streaming copy bandwidth, bounds
-    the filters' kernels."""
+def config_random(args):
+    """The GPU's random-access ceilings, the filters' regime, measured by this
+    library's own kernel (pg_diag_random_access): random 32-byte sectors, random
+    64-byte pairs of sectors, a sector read followed by a CAS on it (an insert's
+    claim), and atomic adds with no return (write-only read-modify-writes), at
+    the filters' table sizes (512 MiB = the tags of a 2^28-slot TCF, 1 GiB =
+    its tags and values, 8 GiB = a 2^32-slot tag-only filter).  Several
+    accesses are in flight per thread; CUDA-event timed, best of 5 after a
+    warm-up, over 4 and 8 blocks of 256 threads per SM."""
     import torch
-    g = torch.Generator(device="cuda")
-    g.manual_seed(5)
-    buf = torch.randint(0, 1 << 62, (1 << 29,), dtype=torch.int64, device="cuda", generator=g)  # 4 GiB
-    n = 1 << 27
-    idx = torch.randint(0, buf.numel(), (n,), dtype=torch.int64, device="cuda", generator=g)
-    out = torch.empty(n, dtype=torch.int64, device="cuda")
-    best = None
-    for _ in range(6):
-        e = _events(2)
-        e[0].record()
-        torch.index_select(buf, 0, idx, out=out)
-        e[1].record()
-        torch.cuda.synchronize()
-        ms = e[0].elapsed_time(e[1])
-        best = ms if best is None else min(best, ms)
-    g_per_s = n / best / 1e6
-    return {"config": "gather", "buffer_bytes": buf.numel() * 8, "reads": n, "ms": round(best, 3),
-            "random_sector_reads_g_per_s": round(g_per_s, 2), "sector_gbs": round(g_per_s * 32, 1),
-            "note": "each read also streams its 8-byte index and writes 8 bytes"}
+    modes = {"read32": pg.PG_DIAG_READ32, "read64": pg.PG_DIAG_READ64, "read32_cas": pg.PG_DIAG_READ32_CAS,
+             "red32": pg.PG_DIAG_RED32}
+    sectors = {"read32": 1, "read64": 2, "read32_cas": 1, "red32": 1}
+    out = {"config": "random", "note": "G accesses/s; sector_g_per_s counts the 32-byte sectors read per access"}
+    sink = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for log2_bytes in (29, 30, 33):
+        buf = torch.zeros(1 << log2_bytes, dtype=torch.uint8, device="cuda")
+        res = {}
+        for name, mode in modes.items():
+            best = None
+            for bps in (4, 8):
+                for rep in range(6):
+                    e = _events(2)
+                    e[0].record()
+                    done = pg.diag_random_access(buf, mode, 1 << 27, seed=rep + 1, blocks_per_sm=bps, sink=sink)
+                    e[1].record()
+                    torch.cuda.synchronize()
+                    if rep == 0:
+                        continue
+                    rate = done / e[0].elapsed_time(e[1]) / 1e6
+                    if best is None or rate > best[0]:
+                        best = (rate, bps)
+            res[name] = {"g_per_s": round(best[0], 2), "sector_g_per_s": round(best[0] * sectors[name], 2),
+                         "sector_gbs": round(best[0] * sectors[name] * 32, 1), "blocks_per_sm": best[1]}
+        out[f"buffer_{(1 << log2_bytes) >> 20}MiB"] = res
+        del buf
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "gather"], required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "random"], required=True)
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--only", nargs="+", default=None, help="config tcf: run only these workloads")
+    ap.add_argument("--tcf-log2", type=int, default=0, help="config tcf: log2 slots instead of each workload's own")
     ap.add_argument("--tables", type=int, default=1024)
     ap.add_argument("--bucket", type=int, default=16)
     ap.add_argument("--lanes", type=int, default=1)
@@ -719,7 +737,7 @@ def main():
     import torch
     torch.cuda.init()
     fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del, "tcf": config_tcf,
-          "gather": config_gather}[a.config]
+          "random": config_random}[a.config]
     print(json.dumps(fn(a)))
 
 

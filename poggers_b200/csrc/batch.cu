@@ -91,15 +91,29 @@ static __device__ __align__(256) unsigned char g_batch_static[sizeof(static_scra
 
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mu;
-void *g_static_addr[kMaxDevices];      // device address of g_batch_static, per device
-table_desc g_static_stage[kStaticMaxTables];  // host staging of the descriptors (guarded by g_static_mu)
+// Device address of g_batch_static, per device ordinal, looked up once.  A
+// cudaDeviceReset() frees the array with the context, so these addresses do not
+// survive one: the entry point must not be used across a device reset.
+void *g_static_addr[kMaxDevices];
 
-// The symbol's device address on the current device; the first call on each
-// device looks it up (cudaGetSymbolAddress, with that device current).
-pg_status static_scratch_addr(static_scratch **out)
+// The descriptors reach the device array as kernel parameters (copied when the
+// launch is enqueued), so no host buffer has to outlive the call.
+constexpr uint32_t kStageChunk = 3840 / sizeof(table_desc);
+static_assert(kStageChunk >= 1, "a table descriptor must fit in a kernel's parameters");
+struct stage_chunk {
+    table_desc d[kStageChunk];
+};
+
+__global__ void k_stage_tables(table_desc *dst, stage_chunk c, uint32_t n)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PG_ERR_CUDA;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.d[i];
+}
+
+// The symbol's device address on device `dev` (the current device); the first
+// call on each device looks it up (cudaGetSymbolAddress, with that device current).
+pg_status static_scratch_addr(int dev, static_scratch **out)
+{
+    if (dev < 0 || dev >= kMaxDevices) return PG_ERR_CUDA;
     if (!g_static_addr[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_batch_static) != cudaSuccess || !p) {
@@ -251,17 +265,22 @@ pg_status pg_batch_run_static(pg_table *const *tables, uint32_t ntables, const p
         const pg_table *t = tables[i];
         if (!same_kernel(t, t0)) return PG_ERR_UNSUPPORTED;
     }
+    // the array and the kernels live on the current device: it must be the tables'
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PG_ERR_CUDA;
+    if (dev != t0->device) return PG_ERR_INVALID;
     std::lock_guard<std::mutex> g(g_static_mu);
     static_scratch *sc = nullptr;
-    pg_status st = static_scratch_addr(&sc);
+    pg_status st = static_scratch_addr(dev, &sc);
     if (st != PG_OK) return st;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    // the descriptors go through a fixed host array; a copy from pageable
-    // memory returns once the source has been read, so the array can be reused
-    for (uint32_t i = 0; i < ntables; i++) g_static_stage[i] = tables[i]->desc;
-    if (cudaMemcpyAsync(sc->tables, g_static_stage, sizeof(table_desc) * ntables, cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
-        return PG_ERR_CUDA;
+    for (uint32_t i = 0; i < ntables; i += kStageChunk) {
+        const uint32_t m = ntables - i < kStageChunk ? ntables - i : kStageChunk;
+        stage_chunk c;
+        for (uint32_t j = 0; j < m; j++) c.d[j] = tables[i + j]->desc;
+        k_stage_tables<<<1, 32, 0, s>>>(sc->tables + i, c, m);
+        if (cudaGetLastError() != cudaSuccess) return PG_ERR_CUDA;
+    }
     batch_args a;
     a.tables = sc->tables;
     a.ops = d_ops;

@@ -1,5 +1,7 @@
 // bulk_kv64_fp.cu -- bulk kernels for uint64 tables with a fingerprint index
 // (one lane per key, bucket_insert primary level; see level_ops_fp).
+#include <mutex>
+
 #include "bulk_kernels.cuh"
 
 namespace pg {
@@ -93,26 +95,32 @@ __global__ void __launch_bounds__(256) k_query_fp_refill(table_desc t, bulk_args
 }
 
 // resident 256-thread blocks of a kernel on the current device (0 if unknown);
-// looked up once per kernel
+// looked up once per (device, kernel), under a lock so host threads may launch
+// concurrently
 int refill_blocks(const void *fn)
 {
-    static const void *keys[8];
-    static int vals[8];
-    for (int k = 0; k < 8; ++k)
-        if (keys[k] == fn) return vals[k];
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+    struct entry {
+        const void *fn;
+        int dev, blocks;
+    };
+    static std::mutex mu;
+    static entry cache[32];
+    static int used = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    for (int k = 0; k < used; ++k)
+        if (cache[k].fn == fn && cache[k].dev == dev) return cache[k].blocks;
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm <= 0) {
         cudaGetLastError();
         return 0;
     }
-    for (int k = 0; k < 8; ++k)
-        if (!keys[k]) {
-            vals[k] = sms * per_sm;
-            keys[k] = fn;
-            break;
-        }
+    if (used < 32) cache[used++] = entry{fn, dev, sms * per_sm};
     return sms * per_sm;
 }
 

@@ -7,12 +7,15 @@
 // this library's namespace, and the kernels follow that test's drivers
 // (delete_tests.cu:248-460): one tile per key, insert, remove the first half,
 // query the second half, re-add the first half with insert_with_delete, then
-// insert_if_not_exists over present keys.  Prints one JSON line of counters.
+// insert_if_not_exists over present keys.  The filters are sized by that
+// test's own generate_size (delete_tests.cu:771-779, a variadic_size of the
+// primary and a 1 % backing level), spelled as there through the compat
+// header's poggers namespace.  Prints one JSON line of counters.
 #include <cstdio>
 #include <cstdint>
 #include <vector>
 #include <cuda_runtime.h>
-#include "poggers_b200/tables.cuh"
+#include "poggers_b200/compat.cuh"
 
 namespace pb = poggers_b200;
 namespace pr = pb::representations;
@@ -107,11 +110,22 @@ static uint64_t splitmix(uint64_t seed, uint64_t i)
 
 // counters: 0 insert fails, 1 delete misses, 2 query misses, 3 query wrong values,
 // 4 re-add fails, 5 if_not_exists not found, 6 if_not_exists failed
-template <class Filter, class Val>
-static int run(const char *name, uint64_t nslots, unsigned long long *bad, bool last)
+__host__ poggers::sizing::variadic_size generate_size(int nbits)
 {
-    pb::sizing::size_in_num_slots<2> size(nslots, nslots / 100);
+    uint64_t nslots = (1ULL << nbits);
+
+    poggers::sizing::variadic_size internal_size(nslots, nslots / 100);
+
+    return internal_size;
+}
+
+template <class Filter, class Val>
+static int run(const char *name, int nbits, unsigned long long *bad, bool last)
+{
+    const uint64_t nslots = 1ULL << nbits;
+    poggers::sizing::variadic_size size = generate_size(nbits);
     Filter *f = Filter::generate_on_device(&size, 42);
+    const uint64_t num_slots = f->get_num_slots(), local_slots = f->get_local_num_slots();
     const uint64_t n = (uint64_t)(0.9 * (nslots + nslots / 100)), half = n / 2;
     std::vector<uint64_t> hk(n);
     std::vector<Val> hv(n);
@@ -146,9 +160,11 @@ static int run(const char *name, uint64_t nslots, unsigned long long *bad, bool 
     cudaFree(dv);
     printf("\"%s\": {\"keys\": %llu, \"insert_fail\": %llu, \"delete_miss\": %llu, \"query_miss\": %llu, "
            "\"query_wrong_val\": %llu, \"readd_fail\": %llu, \"ine_not_found\": %llu, \"ine_fail\": %llu, "
-           "\"fill_before\": %llu, \"fill_after_delete\": %llu, \"fill_final\": %llu, \"cuda\": %d}%s\n",
+           "\"fill_before\": %llu, \"fill_after_delete\": %llu, \"fill_final\": %llu, \"num_slots\": %llu, "
+           "\"local_num_slots\": %llu, \"cuda\": %d}%s\n",
            name, (unsigned long long)n, h[0], h[1], h[2], h[3], h[4], h[5], h[6], (unsigned long long)fill_before,
-           (unsigned long long)fill_after, (unsigned long long)fill_final, (int)e, last ? "" : ",");
+           (unsigned long long)fill_after, (unsigned long long)fill_final, (unsigned long long)num_slots,
+           (unsigned long long)local_slots, (int)e, last ? "" : ",");
     return e == cudaSuccess ? 0 : 1;
 }
 
@@ -157,8 +173,8 @@ int main()
     unsigned long long *bad;
     cudaMalloc(&bad, 8 * sizeof(unsigned long long));
     printf("{\n");
-    int rc = run<del_TCF, uint16_t>("del_TCF", 1ULL << 20, bad, false);
-    rc |= run<del_TCF_small, uint8_t>("del_TCF_small", 1ULL << 20, bad, true);
+    int rc = run<del_TCF, uint16_t>("del_TCF", 20, bad, false);
+    rc |= run<del_TCF_small, uint8_t>("del_TCF_small", 20, bad, true);
     printf("}\n");
     cudaFree(bad);
     return rc;

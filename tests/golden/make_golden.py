@@ -193,7 +193,7 @@ def ht_exceptions(okn, vals, half, rem_idx, found, vv, rok, found2, vv2):
     """Compare one run's query / remove results with what its own insert report
     implies (a key is present iff its insert succeeded and it was not removed;
     a present key returns its value).  Every index that disagrees is listed."""
-    n_q = 2 * half
+    n_q = len(found)  # the first `half` queries are inserted keys, the rest absent
     exp_f = np.zeros(n_q, dtype=bool)
     exp_f[:half] = okn[:half]
     exp_v = np.zeros(n_q, dtype=np.uint64)

@@ -50,6 +50,9 @@ def test_bucketed_table_device_api(drivers):
         assert c["fill_final"] == c["fill_after_delete"] + half - c["readd_fail"]
         # every key is present after the re-add, so insert_if_not_exists finds it
         assert c["ine_fail"] == 0 and c["ine_not_found"] <= 20, (name, c)
+        # sized by variadic_size(2^20, 2^20 / 100): 2^16 buckets of 16 slots and
+        # ceil(10485 / 8) buckets of 8 slots
+        assert c["local_num_slots"] == 1 << 20 and c["num_slots"] == (1 << 20) + 1311 * 8, (name, c)
 
 
 def test_slab_allocator_device_api(drivers):

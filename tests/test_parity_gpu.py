@@ -163,21 +163,47 @@ def _load_stats():
     return json.loads(p.read_text())
 
 
-def test_full_size_ht_workload_matches_reference(pg):
-    """2^26 slots at 0.9 load: every query and remove result agrees with the run's
-    own insert report (zero exceptions, like the reference's recorded run), and
-    the failure counts are of the reference's order."""
-    import torch
-    from tests.golden.make_golden import ht_exceptions
-    stats = _load_stats()
-    nslots = 1 << 26
-    n = int(0.9 * nslots)
-    keys = wl.keys_without_sentinels(43, n)
-    vals = wl.values_for(keys, 8, 50)
-    half = n // 2
-    qkeys = np.concatenate([keys[:half], wl.keys_without_sentinels(4343, half)])
+@pytest.fixture(scope="module")
+def full_size_ht_oracle(oracle):
+    """The benchmarked workload (2^26 slots, bucket 8, 20 double-hash probes,
+    0.9 load; half of the queries absent; a seeded random half removed, then
+    every query repeated) run through the sequential oracle, one key at a time
+    in batch order (bucket_insert.cuh:127-357).  Queries and removes of
+    distinct keys do not depend on their order, so those run on 8 threads."""
+    import bench
+    keys, vals, qkeys = bench.make_inputs()
+    n = len(keys)
     rem_idx = wl.fisher_yates_half(n, 77)
-    t = pg.Table(pg.data_structs.hash_table_64(nslots, bucket=8), 43)
+    o = oracle.OracleTable(0, bench.TILE, [(bench.NSLOTS, bench.BUCKET, bench.PROBES, 0, 0)], bench.SEED)
+    ok = o.insert_many(keys, vals)
+    f, v = o.query_many(qkeys, threads=8)
+    r = o.remove_many(keys[rem_idx], threads=8)
+    f2, v2 = o.query_many(qkeys, threads=8)
+    return dict(keys=keys, vals=vals, qkeys=qkeys, rem_idx=rem_idx, ok=ok, f=f, v=v, r=r, f2=f2, v2=v2)
+
+
+@pytest.mark.parametrize("insert_order", ["region", "batch"])
+@pytest.mark.parametrize("layout", ["fingerprints", "interleaved"])
+def test_full_size_ht_workload_matches_reference(pg, full_size_ht_oracle, layout, insert_order):
+    """The benchmarked path at its full size: bench.py's own table setup (2^26
+    slots, bucket 8, tile 4, 20 double-hash probes, its launch shape; the
+    fingerprint layout with region-ordered inserts and the lane-refill query is
+    what bench.py times).  Every query, remove and re-query result is
+    bit-exact against the sequential oracle on every key that both runs placed,
+    and agrees with the run's own insert report (zero exceptions, like the
+    reference's recorded run, whose 125 insert failures bound ours)."""
+    import torch
+    import bench
+    from tests.golden.make_golden import ht_exceptions
+    o = full_size_ht_oracle
+    keys, vals, qkeys, rem_idx = o["keys"], o["vals"], o["qkeys"], o["rem_idx"]
+    n = len(keys)
+    half = n // 2
+    cfg = pg.data_structs.hash_table_64(bench.NSLOTS, tile=bench.TILE, bucket=bench.BUCKET, max_probes=bench.PROBES)
+    cfg.fingerprints = layout == "fingerprints"
+    t = pg.Table(cfg, bench.SEED)
+    t.set_launch(bench.BLOCK_THREADS, bench.BLOCKS_PER_SM, 0, bench.LANES)
+    t.set_partitioned_insert(insert_order == "region")
     d = Driver(t)
     ok = d.insert(keys, vals)
     f, v = d.query(qkeys)
@@ -187,14 +213,22 @@ def test_full_size_ht_workload_matches_reference(pg):
     assert res["n_query_exceptions"] == 0
     assert res["n_remove_exceptions"] == 0
     assert res["n_requery_exceptions"] == 0
-    assert len(res["insert_failed"]) < 2000
-    if stats is not None:
-        ref = stats["ht"]
-        assert ref["n_query_exceptions"] == 0 and ref["n_requery_exceptions"] == 0
-        # keys both runs placed: found counts agree exactly
-        both_failed = set(ref["insert_failed"]) | set(res["insert_failed"])
-        assert abs(len(res["insert_failed"]) - len(ref["insert_failed"])) <= max(50, len(ref["insert_failed"]))
-        assert abs(res["found"] - ref["found"]) <= len(both_failed)
+    # the reference's own parallel build failed 125 of these inserts, the
+    # sequential oracle 119; which ones fail depends on the order of the CASes,
+    # so the count is a random variable: within three standard deviations
+    # (Poisson) of the reference's
+    stats = _load_stats()
+    ref_failed = len(stats["ht"]["insert_failed"]) if stats is not None else 125
+    nfail = int((~ok).sum())
+    assert nfail <= ref_failed + 3 * ref_failed ** 0.5, f"{nfail} insert failures, reference {ref_failed}"
+    # bit-exact against the oracle on every key both runs placed
+    both = ok & o["ok"]
+    qboth = np.concatenate([both[:half], np.ones(len(qkeys) - half, dtype=bool)])
+    assert (f[qboth] == o["f"][qboth]).all() and (v[qboth] == o["v"][qboth]).all()
+    assert (v[:half][ok[:half]] == vals[:half][ok[:half]]).all()
+    rboth = both[rem_idx]
+    assert (r[rboth] == o["r"][rboth]).all()
+    assert (f2[qboth] == o["f2"][qboth]).all() and (v2[qboth] == o["v2"][qboth]).all()
     del t
     torch.cuda.empty_cache()
 
