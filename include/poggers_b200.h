@@ -295,6 +295,11 @@ typedef struct pg_batch pg_batch;
 pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t max_ops, pg_batch **out);
 pg_status pg_batch_destroy(pg_batch *b);
 pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t lanes_per_key);
+/* Clear every table of the batch (what pg_table_clear does to each: all levels
+ * and fingerprint arrays zeroed) with one kernel launch, so a captured graph of
+ * a whole batch step holds one clear instead of a memset per table and level.
+ * No counterpart in the reference. */
+pg_status pg_batch_clear(pg_batch *b, pg_stream_t stream);
 /* Run d_ops[0 .. *d_nops) (both device memory, so one captured CUDA graph can be
  * replayed with new requests).  Keys, values and per-key flags are indexed by
  * the requests' offsets; d_op_counts[j] (optional) += hits of query / remove

@@ -60,6 +60,11 @@ enum fmt_kind : uint32_t {
 enum scheme_kind : uint32_t { SCHEME_BUCKET = 0, SCHEME_TWO_CHOICE = 1 };
 
 constexpr int kTwoChoiceMaxProbes = 4;
+#ifndef PG_TWO_CHOICE_PREFETCH
+#define PG_TWO_CHOICE_PREFETCH 1
+#endif
+// read a two-choice key's second bucket together with its first (see insert_two_choice)
+constexpr bool kTwoChoicePrefetch = PG_TWO_CHOICE_PREFETCH != 0;
 
 struct level_desc {
     unsigned char *base;   // bucket array
@@ -380,7 +385,11 @@ struct level_ops {
 
     // ---- insert: two-choice shortcut (power_of_n_shortcut.cuh:327-435).
     // Probe bookkeeping is unrolled over kTwoChoiceMaxProbes so it stays in
-    // registers; both choices of the common 2-probe case are fetched together.
+    // registers.  With kTwoChoicePrefetch both choices of the common 2-probe
+    // case are fetched together (one round trip, two random sectors for every
+    // key); without it the second choice is read only when the first is at or
+    // above the shortcut threshold (a second round trip for those keys, one
+    // sector fewer for the others).
     __device__ static bool insert_two_choice(const level_desc &L, const group<G> &g, uint64_t key, V val)
     {
         const K sk = F::stored(key);
@@ -392,7 +401,7 @@ struct level_ops {
         int np = 0, min_fill = B;
         snap k1;
         bool act1 = false, have1 = false;
-        if (L.max_probes >= 2 && ps.at(0) != kProbeEnd && ps.at(1) != kProbeEnd) {
+        if (kTwoChoicePrefetch && L.max_probes >= 2 && ps.at(0) != kProbeEnd && ps.at(1) != kProbeEnd) {
             load(L, g, L.nbmod.mod(ps.at(1)), k1, act1);
             have1 = true;
         }
@@ -498,7 +507,9 @@ struct level_ops {
         uint64_t b1 = 0;
         bool two = L.max_probes >= 2 && ps.at(1) != kProbeEnd;
         load(L, g, b0, k0, a0);
-        if (two) {
+        // the first match in probe order answers: the second choice is read
+        // with the first (kTwoChoicePrefetch) or only after the first missed
+        if (kTwoChoicePrefetch && two) {
             b1 = L.nbmod.mod(ps.at(1));
             load(L, g, b1, k1, a1);
         }
@@ -508,6 +519,10 @@ struct level_ops {
             return true;
         }
         if (!two) return false;
+        if (!kTwoChoicePrefetch) {
+            b1 = L.nbmod.mod(ps.at(1));
+            load(L, g, b1, k1, a1);
+        }
         fm = first(g, a1 ? eq_mask(k1.k, sk) : 0u);
         if (fm >= 0) {
             out = read_val(L, g, b1, fm, k1);

@@ -220,6 +220,13 @@ __device__ __forceinline__ bool slab_release(const slab_desc &S, const void *p)
     return true;
 }
 
+// Any thread may call it, from any branch (the reference's per-thread
+// malloc()).  The lanes of a warp that reach the call together form the group:
+// lanes converged at an __activemask() call all receive the same mask, and a
+// lane that arrives separately receives a mask without the others.  Every
+// warp-synchronizing call in slab_claim names exactly that mask, and its
+// control flow is uniform over the group (loop bounds and branches come from
+// values broadcast by the leader), so the group's lanes meet at each one.
 __device__ __forceinline__ void *slab_malloc(const slab_desc &S)
 {
     const uint64_t off = slab_claim(S, __activemask());

@@ -82,6 +82,14 @@ class RefTable:
         if r != 0:
             raise RuntimeError("refc_bbulk launch failed")
 
+    # bytes of one bucket per level for the kinds whose levels time_refcuda clears
+    # (data_structs::tcf: 16 slots of 4 bytes, backed by tiny_static_table_4's
+    # 4 slots of 4 bytes; the 8-slot uint64 table: 8 slots of 16 bytes)
+    _BUCKET_BYTES = {KIND_TCF: (64, 16), KIND_TCQF: (32,), KIND_HT_DOUBLE_B8: (128,)}
+
+    def bucket_bytes(self, level: int) -> int:
+        return self._BUCKET_BYTES[self.kind][level]
+
     def level(self, level: int):
         p = C.c_void_p()
         nb = C.c_uint64()

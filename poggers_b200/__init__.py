@@ -91,6 +91,7 @@ EXPORTED = (
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_desc", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
     "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
+    "pg_batch_clear",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
     "pg_diag_random_access",
@@ -187,6 +188,8 @@ def lib() -> C.CDLL:
     L.pg_batch_set_launch.argtypes = [V, U32, U32, U32]
     L.pg_batch_run.restype = C.c_int
     L.pg_batch_run.argtypes = [V, P, P, P, P, P, P, P, P]
+    L.pg_batch_clear.restype = C.c_int
+    L.pg_batch_clear.argtypes = [V, P]
     L.pg_batch_run_static.restype = C.c_int
     L.pg_batch_run_static.argtypes = [C.POINTER(V), U32, P, P, U32, P, P, P, P, P, P]
     L.pg_server_create.restype = C.c_int
@@ -668,6 +671,10 @@ class Batch:
 
     def set_launch(self, block_threads: int = 0, blocks_per_sm: int = 0, lanes_per_key: int = 0) -> None:
         _check(lib().pg_batch_set_launch(self._h, block_threads, blocks_per_sm, lanes_per_key), "pg_batch_set_launch")
+
+    def clear(self, stream=None) -> None:
+        """Clear every table of the batch with one kernel (pg_batch_clear)."""
+        _check(lib().pg_batch_clear(self._h, _stream(stream)), "pg_batch_clear")
 
     def run(self, ops, nops, keys, vals_in=None, vals_out=None, flags=None, op_counts=None, stream=None) -> None:
         """ops: int64 device tensor from pack_ops; nops: int32 device tensor holding the request count."""

@@ -14,6 +14,16 @@ the device over
 
 and returns the fastest shape.  Results are cached per GPU and table shape in
 a JSON file so a serving process pays for the sweep once.
+
+The multi-table batch path (pg_batch_run over many tables of uneven size) has
+its own sweep: lanes per key (1, 2, 4, 8, 16), bucket size (8, 16, 32: a
+different table, built once per bucket size) and resident blocks per SM, each
+shape timed as replays of one captured CUDA graph holding the batch's insert
+run and query run, with the batch cleared by one kernel between replays.
+The pick is the fastest shape among those whose insert failures are within
+a small margin of the fewest any shape had (small two-choice tables fail
+more keys when too many of their keys are in flight at once).  Cached per GPU
+and size class of the batch.
 """
 from __future__ import annotations
 
@@ -126,3 +136,106 @@ def tuned_shape(config, seed: int, keys, vals, qkeys, **grid) -> Shape:
     CACHE.parent.mkdir(parents=True, exist_ok=True)
     CACHE.write_text(json.dumps(cache, indent=1))
     return b.shape
+
+
+# ---------------------------------------------------------------- batch path
+@dataclass
+class BatchShape:
+    lanes: int
+    bucket: int
+    blocks_per_sm: int
+    block_threads: int = 256
+
+
+@dataclass
+class BatchResult:
+    shape: BatchShape
+    step_ms: float        # one graph replay: every insert request, then every query request
+    insert_failures: int
+
+
+def _batch_ok(results: list[BatchResult]) -> list[BatchResult]:
+    fewest = min(r.insert_failures for r in results)
+    bound = fewest + max(16, fewest // 2)
+    return [r for r in results if r.insert_failures <= bound]
+
+
+def best_batch(results: list[BatchResult]) -> BatchResult:
+    return min(_batch_ok(results), key=lambda r: r.step_ms)
+
+
+def sweep_batch(make_configs, seeds, ins_ops, q_ops, nops, keys, vals, qkeys, lanes=(1, 2, 4, 8, 16),
+                buckets=(8, 16, 32), blocks_per_sm=(4, 8, 16), reps: int = 3) -> list[BatchResult]:
+    """Time every batch shape.  make_configs(bucket) -> one TableConfig per
+    table; ins_ops / q_ops are device request arrays (pack_ops) over keys /
+    qkeys, nops a device int32 holding the request count."""
+    import torch
+    import poggers_b200 as pg
+
+    out = []
+    n = keys.numel()
+    ok = torch.zeros(n, dtype=torch.uint8, device=keys.device)
+    found = torch.zeros(qkeys.numel(), dtype=torch.uint8, device=keys.device)
+    s = torch.cuda.Stream()
+    for bucket in buckets:
+        tables = [pg.Table(c, sd) for c, sd in zip(make_configs(bucket), seeds)]
+        batch = pg.Batch(tables, max_ops=max(1, len(tables)))
+        for ln, bps in itertools.product(lanes, blocks_per_sm):
+            if ln > bucket:
+                continue
+            try:
+                batch.set_launch(256, bps, ln)
+            except pg.PoggersError:
+                continue
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                batch.clear(s)
+                batch.run(ins_ops, nops, keys, vals, None, ok, None, s)
+                batch.run(q_ops, nops, qkeys, None, None, found, None, s)
+            s.synchronize()
+            with torch.cuda.graph(g, stream=s):
+                batch.run(ins_ops, nops, keys, vals, None, ok, None, s)
+                batch.run(q_ops, nops, qkeys, None, None, found, None, s)
+            times = []
+            for _ in range(reps + 1):
+                with torch.cuda.stream(s):
+                    batch.clear(s)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(s)
+                    g.replay()
+                    e1.record(s)
+                s.synchronize()
+                times.append(e0.elapsed_time(e1))
+            fails = int((ok == 0).sum().item())
+            out.append(BatchResult(BatchShape(ln, bucket, bps), float(np.median(times[1:])), fails))
+            del g
+        batch.free()
+        for t in tables:
+            t.free_on_device()
+    return out
+
+
+def batch_cache_key(gpu_name: str, configs) -> str:
+    c0 = configs[0]
+    L = c0.levels[0]
+    lo = min(c.levels[0].nslots for c in configs).bit_length()
+    hi = max(c.levels[0].nslots for c in configs).bit_length()
+    return (f"{gpu_name}|batch|fmt{c0.format}|s{L.scheme}|p{L.probe}|lv{len(c0.levels)}|t{len(configs).bit_length()}"
+            f"|n{lo}-{hi}")
+
+
+def tuned_batch_shape(make_configs, seeds, ins_ops, q_ops, nops, keys, vals, qkeys, **grid):
+    """The cached best batch shape for this GPU and size class, sweeping on a
+    miss.  Returns (shape, results of the sweep or None when cached)."""
+    import torch
+    key = batch_cache_key(torch.cuda.get_device_name(), make_configs(16))
+    cache = json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    if key in cache:
+        return BatchShape(**cache[key]["shape"]), None
+    res = sweep_batch(make_configs, seeds, ins_ops, q_ops, nops, keys, vals, qkeys, **grid)
+    b = best_batch(res)
+    cache[key] = {"shape": asdict(b.shape), "step_ms": b.step_ms, "insert_failures": b.insert_failures,
+                  "when": time.time()}
+    CACHE.parent.mkdir(parents=True, exist_ok=True)
+    CACHE.write_text(json.dumps(cache, indent=1))
+    return b.shape, res

@@ -100,20 +100,13 @@ def config1(args):
 
 
 # ---------------------------------------------------------------- config 3
-def config3(args):
-    """1024 TCFs, slot counts log-uniform in [2^12, 2^20], each filled to 0.9.
-    All inserts in one batched launch, then all queries (half inserted, half
-    absent) in another, replayed from a captured CUDA graph; against 1024
-    per-table launches per phase."""
-    import torch
-    rng = np.random.default_rng(3)
-    ntab = args.tables
+def config3_inputs(ntab: int, seed: int = 3):
+    """1024 TCF shapes with slot counts log-uniform in [2^12, 2^20] and a 1 %
+    backing level (as the plain TCF), each filled to 0.9 with its own keys; the
+    queries are half the table's keys, half never inserted."""
+    rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 20), ntab)).astype(np.int64)
-    bucket = args.bucket
-    tables = []
-    for i, n in enumerate(sizes):
-        cfg = pg.data_structs.tcf(int(n), max(int(n) // 20, 64), bucket=bucket)
-        tables.append(pg.Table(cfg, 1000 + i))
+    backing = [max(int(n) // 100, 64) for n in sizes]
     counts = (0.9 * sizes).astype(np.int64)
     keys = [wl.keys_without_sentinels(77_000 + i, int(c)) for i, c in enumerate(counts)]
     qkeys = [np.concatenate([k[: len(k) // 2], wl.keys_without_sentinels(99_000 + i, len(k) - len(k) // 2)])
@@ -121,19 +114,48 @@ def config3(args):
     ins_all, q_all = np.concatenate(keys), np.concatenate(qkeys)
     offs = np.concatenate([[0], np.cumsum(counts)])
     vals = wl.values_for(ins_all, 2, 5)
-    dk, dv, dq = _dev(ins_all), _dev(vals), _dev(q_all)
-    N = len(ins_all)
+    return {"sizes": sizes, "backing": backing, "counts": counts, "offs": offs, "ins": ins_all, "q": q_all,
+            "vals": vals, "seeds": [1000 + i for i in range(ntab)]}
+
+
+def config3(args):
+    """1024 TCFs, slot counts log-uniform in [2^12, 2^20], each filled to 0.9.
+    The batched path runs all inserts in one persistent run, then all queries
+    (half inserted, half absent) in another, replayed from one captured CUDA
+    graph, in the shape the autotuner picks (lanes per key x bucket size x
+    blocks per SM); against 1024 per-table launches per phase on the same
+    tables.  Tables are cleared (one kernel) before every timed step, outside
+    the timed region, for both paths."""
+    import torch
+    from poggers_b200 import autotune as at
+    ntab = args.tables
+    d = config3_inputs(ntab)
+    sizes, counts, offs = d["sizes"], d["counts"], d["offs"]
+    dk, dv, dq = _dev(d["ins"]), _dev(d["vals"]), _dev(d["q"])
+    N = len(d["ins"])
+    ins_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_INSERT, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
+    q_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_QUERY, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
+    d_n = torch.tensor([ntab], dtype=torch.int32, device="cuda")
+
+    def make_configs(bucket):
+        return [pg.data_structs.tcf(int(n), b, bucket=bucket) for n, b in zip(sizes, d["backing"])]
+
+    grid = {}
+    if args.lanes_grid:
+        grid["lanes"] = tuple(args.lanes_grid)
+    if args.bucket_grid:
+        grid["buckets"] = tuple(args.bucket_grid)
+    if args.bps_grid:
+        grid["blocks_per_sm"] = tuple(args.bps_grid)
+    shape, sweep_res = at.tuned_batch_shape(make_configs, d["seeds"], ins_ops, q_ops, d_n, dk, dv, dq, **grid)
+    tables = [pg.Table(c, sd) for c, sd in zip(make_configs(shape.bucket), d["seeds"])]
     ok = torch.zeros(N, dtype=torch.uint8, device="cuda")
     found = torch.zeros(N, dtype=torch.uint8, device="cuda")
-    lanes = args.lanes
+    batch = pg.Batch(tables, max_ops=ntab)
+    batch.set_launch(shape.block_threads, shape.blocks_per_sm, shape.lanes)
 
-    # plain path: one launch per table per phase
-    for t in tables:
-        t.set_launch(256, 8, 0, lanes)
-
+    # plain path: one launch per table per phase (each table's default launch)
     def plain():
-        for t in tables:
-            t.clear()
         for i, t in enumerate(tables):
             a, b = int(offs[i]), int(offs[i + 1])
             t.bulk_insert(dk[a:b], dv[a:b], ok[a:b])
@@ -141,46 +163,36 @@ def config3(args):
             a, b = int(offs[i]), int(offs[i + 1])
             t.bulk_query(dq[a:b], None, found[a:b])
 
-    # batched path: one run per phase, captured once
-    batch = pg.Batch(tables, max_ops=ntab)
-    batch.set_launch(256, args.blocks_per_sm, lanes)
-    ins_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_INSERT, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
-    q_ops = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_QUERY, int(offs[i]), int(counts[i])) for i in range(ntab)])).cuda()
-    d_n = torch.tensor([ntab], dtype=torch.int32, device="cuda")
     s = torch.cuda.Stream()
-
-    def batched_run(stream):
-        batch.run(ins_ops, d_n, dk, dv, None, ok, None, stream)
-        batch.run(q_ops, d_n, dq, None, None, found, None, stream)
-
-    def clear_all(stream):
-        for t in tables:
-            t.clear(stream)
-
     with torch.cuda.stream(s):
-        clear_all(s)
-        batched_run(s)
-    torch.cuda.synchronize()
+        batch.clear(s)
+        batch.run(ins_ops, d_n, dk, dv, None, ok, None, s)
+        batch.run(q_ops, d_n, dq, None, None, found, None, s)
+    s.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=s):
-        clear_all(s)
-        batched_run(s)
+        batch.run(ins_ops, d_n, dk, dv, None, ok, None, s)
+        batch.run(q_ops, d_n, dq, None, None, found, None, s)
 
     def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        e0, e1 = _events(2)
-        e0.record()
-        for _ in range(reps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+        ms = []
+        for _ in range(reps + 1):
+            with torch.cuda.stream(s):
+                batch.clear(s)
+                e0, e1 = _events(2)
+                e0.record(s)
+                fn()
+                e1.record(s)
+            s.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms[1:]))
 
     plain_ms = timed(plain, args.steps)
     graph_ms = timed(g.replay, args.steps)
-    g.replay()
-    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        batch.clear(s)
+        g.replay()
+    s.synchronize()
     okn = ok.cpu().numpy().astype(bool)
     fnd = found.cpu().numpy().astype(bool)
     fn_total = 0
@@ -193,12 +205,19 @@ def config3(args):
     ops = 2 * N
     del g
     batch.free()
-    return {"config": 3, "workload": f"{ntab} TCFs, slots log-uniform [2^12, 2^20] (total {int(sizes.sum())}), 0.9 load, "
-                                     f"bucket {bucket}, lanes/key {lanes}",
-            "keys": int(N), "plain_ms": round(plain_ms, 3), "batched_graph_ms": round(graph_ms, 3),
-            "plain_mops": round(ops / plain_ms / 1e3, 1), "batched_mops": round(ops / graph_ms / 1e3, 1),
-            "speedup": round(plain_ms / graph_ms, 2), "insert_failures": int((~okn).sum()),
-            "false_negatives": fn_total, "fp_rate": fp_total / max(1, N - N // 2)}
+    out = {"config": 3, "workload": f"{ntab} TCFs, slots log-uniform [2^12, 2^20] (total {int(sizes.sum())}), 1 % "
+                                    "backing, 0.9 load; inserts then queries (half absent)",
+           "tuned_shape": {"lanes_per_key": shape.lanes, "bucket": shape.bucket, "blocks_per_sm": shape.blocks_per_sm,
+                           "block_threads": shape.block_threads},
+           "keys": int(N), "plain_ms": round(plain_ms, 3), "batched_graph_ms": round(graph_ms, 3),
+           "plain_mops": round(ops / plain_ms / 1e3, 1), "batched_mops": round(ops / graph_ms / 1e3, 1),
+           "speedup": round(plain_ms / graph_ms, 2), "insert_failures": int((~okn).sum()),
+           "false_negatives": fn_total, "fp_rate": fp_total / max(1, N - N // 2),
+           "graph_kernels_per_step": 4}
+    if sweep_res is not None:
+        out["sweep"] = [{"lanes": r.shape.lanes, "bucket": r.shape.bucket, "blocks_per_sm": r.shape.blocks_per_sm,
+                         "step_ms": round(r.step_ms, 3), "insert_failures": r.insert_failures} for r in sweep_res]
+    return out
 
 
 # ---------------------------------------------------------------- config 4
@@ -443,7 +462,7 @@ def tcf_phases(run, d):
 
 
 def tcf_summary(runs, d):
-    ms = np.median(np.array([r[0] for r in runs]), axis=0)
+    ms = np.median(np.array([r[0] for r in runs]).reshape(len(runs), -1), axis=0)
     n = d["n"]
     mops = [n / m / 1e3 for m in ms]
     return {"insert_mops": round(mops[0], 1), "query_positive_mops": round(mops[1], 1),
@@ -479,10 +498,11 @@ def config_tcf(args):
                 t.bulk_query(k, None, fl)
 
         runs = []
-        for step in range(args.steps + 2):
+        warm = 2 if args.steps > 0 else 1  # --steps 0: one warm-up and one measured run (profiling captures)
+        for step in range(max(args.steps, 1) + warm):
             t.clear()
             r = tcf_phases(run, d)
-            if step >= 2:
+            if step >= warm:
                 runs.append(r)
         res[name] = tcf_summary(runs, d)
         del t, d
@@ -686,14 +706,16 @@ def config_random(args):
     the filters' table sizes (512 MiB = the tags of a 2^28-slot TCF, 1 GiB =
     its tags and values, 8 GiB = a 2^32-slot tag-only filter).  Several
     accesses are in flight per thread; CUDA-event timed, best of 5 after a
-    warm-up, over 4 and 8 blocks of 256 threads per SM."""
+    warm-up, over 4 and 8 blocks of 256 threads per SM.  A 32 MiB buffer,
+    which stays in L2, gives the L2's own rates for the same accesses (the
+    uint64 table's fingerprint words live there)."""
     import torch
     modes = {"read32": pg.PG_DIAG_READ32, "read64": pg.PG_DIAG_READ64, "read32_cas": pg.PG_DIAG_READ32_CAS,
              "red32": pg.PG_DIAG_RED32}
     sectors = {"read32": 1, "read64": 2, "read32_cas": 1, "red32": 1}
     out = {"config": "random", "note": "G accesses/s; sector_g_per_s counts the 32-byte sectors read per access"}
     sink = torch.zeros(1, dtype=torch.int64, device="cuda")
-    for log2_bytes in (29, 30, 33):
+    for log2_bytes in (25, 29, 30, 33):  # 32 MiB stays in L2: the L2's own rates
         buf = torch.zeros(1 << log2_bytes, dtype=torch.uint8, device="cuda")
         res = {}
         for name, mode in modes.items():
@@ -726,6 +748,9 @@ def main():
     ap.add_argument("--only", nargs="+", default=None, help="config tcf: run only these workloads")
     ap.add_argument("--tcf-log2", type=int, default=0, help="config tcf: log2 slots instead of each workload's own")
     ap.add_argument("--tables", type=int, default=1024)
+    ap.add_argument("--lanes-grid", type=int, nargs="+", default=None, help="config 3: the tuner's lanes per key")
+    ap.add_argument("--bucket-grid", type=int, nargs="+", default=None, help="config 3: the tuner's bucket sizes")
+    ap.add_argument("--bps-grid", type=int, nargs="+", default=None, help="config 3: the tuner's blocks per SM")
     ap.add_argument("--bucket", type=int, default=16)
     ap.add_argument("--lanes", type=int, default=1)
     ap.add_argument("--blocks-per-sm", type=int, default=8)

@@ -19,6 +19,13 @@ struct pg_batch {
     uint32_t bucket1;  // backing level's bucket size (the bucketed filter's kernels take it as a parameter)
     bool backing;
     table_desc *d_tables;
+    // pg_batch_clear: the device ranges of every level and fingerprint array of
+    // the batch's tables, and the running sum of their bytes
+    uint32_t nseg;
+    unsigned char **d_seg_ptr;
+    unsigned long long *d_seg_bytes;
+    unsigned long long *d_seg_end;  // inclusive prefix of the segments' spans rounded up to 16 bytes
+    unsigned long long clear_padded;
     unsigned long long *d_scratch;  // chunk_start[max_ops + 1] then the work counter
     int num_sms;
     uint32_t block_threads, blocks_per_sm, lanes;
@@ -66,6 +73,36 @@ __global__ void __launch_bounds__(1024) k_batch_plan(batch_args a)
         __syncthreads();
     }
     if (threadIdx.x == 0) a.chunk_start[nops] = carry;
+}
+
+// Zero every segment of a batch.  Each segment's span is rounded up to 16
+// bytes in a global numbering (seg_end: inclusive prefix of the padded spans),
+// so 16-byte chunk j lies inside one segment at an offset that is a multiple
+// of 16; the segment is found by binary search, a full chunk is one 16-byte
+// store (segment bases come from cudaMalloc, so they are aligned), and a
+// segment's last partial chunk is written byte by byte, up to its true size.
+__global__ void __launch_bounds__(256) k_batch_clear(unsigned char *const *seg, const unsigned long long *seg_bytes,
+                                                     const unsigned long long *seg_end, uint32_t nseg,
+                                                     unsigned long long padded_total)
+{
+    const unsigned long long chunks = padded_total / 16;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < chunks;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long byte = j * 16;
+        uint32_t lo = 0, hi = nseg - 1;  // first segment whose padded end is past `byte`
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (seg_end[mid] > byte) hi = mid;
+            else lo = mid + 1;
+        }
+        const unsigned long long off = byte - (lo ? seg_end[lo - 1] : 0ULL);
+        const unsigned long long n = seg_bytes[lo];
+        if (off + 16 <= n) {
+            *reinterpret_cast<uint4 *>(seg[lo] + off) = make_uint4(0, 0, 0, 0);
+        } else {
+            for (unsigned long long q = off; q < n; ++q) seg[lo][q] = 0;
+        }
+    }
 }
 
 }  // namespace pg
@@ -173,9 +210,38 @@ pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t ma
     b->lanes = pg_table_lanes(t0);
     table_desc *h = (table_desc *)malloc(sizeof(table_desc) * ntables);
     for (uint32_t i = 0; i < ntables; i++) h[i] = tables[i]->desc;
+    // the ranges pg_batch_clear zeroes: what pg_table_clear zeroes, for every table
+    const uint32_t maxseg = ntables * 3;
+    unsigned char **sp = (unsigned char **)malloc(sizeof(unsigned char *) * maxseg);
+    unsigned long long *sb = (unsigned long long *)malloc(sizeof(unsigned long long) * maxseg);
+    unsigned long long *se = (unsigned long long *)malloc(sizeof(unsigned long long) * maxseg);
+    uint32_t ns = 0;
+    unsigned long long run = 0;
+    auto add = [&](void *p, uint64_t bytes) {
+        if (!p || !bytes) return;
+        sp[ns] = static_cast<unsigned char *>(p);
+        sb[ns] = bytes;
+        run += (bytes + 15) / 16 * 16;
+        se[ns++] = run;
+    };
+    for (uint32_t i = 0; i < ntables; i++) {
+        for (uint32_t l = 0; l < tables[i]->cfg.nlevels; l++) add(tables[i]->mem[l], tables[i]->bytes[l]);
+        add(tables[i]->fp, tables[i]->fp_bytes);
+    }
+    b->nseg = ns;
+    b->clear_padded = run;
     cudaError_t e = cudaMalloc(&b->d_tables, sizeof(table_desc) * ntables);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_tables, h, sizeof(table_desc) * ntables, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_scratch, sizeof(unsigned long long) * ((uint64_t)max_ops + 2));
+    if (e == cudaSuccess && ns) e = cudaMalloc(&b->d_seg_ptr, sizeof(unsigned char *) * ns);
+    if (e == cudaSuccess && ns) e = cudaMalloc(&b->d_seg_bytes, sizeof(unsigned long long) * ns);
+    if (e == cudaSuccess && ns) e = cudaMalloc(&b->d_seg_end, sizeof(unsigned long long) * ns);
+    if (e == cudaSuccess && ns) e = cudaMemcpy(b->d_seg_ptr, sp, sizeof(unsigned char *) * ns, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ns) e = cudaMemcpy(b->d_seg_bytes, sb, sizeof(unsigned long long) * ns, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ns) e = cudaMemcpy(b->d_seg_end, se, sizeof(unsigned long long) * ns, cudaMemcpyHostToDevice);
+    free(sp);
+    free(sb);
+    free(se);
     free(h);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -191,8 +257,24 @@ pg_status pg_batch_destroy(pg_batch *b)
     if (!b) return PG_ERR_INVALID;
     cudaFree(b->d_tables);
     cudaFree(b->d_scratch);
+    cudaFree(b->d_seg_ptr);
+    cudaFree(b->d_seg_bytes);
+    cudaFree(b->d_seg_end);
     free(b);
     return PG_OK;
+}
+
+pg_status pg_batch_clear(pg_batch *b, pg_stream_t stream)
+{
+    if (!b) return PG_ERR_INVALID;
+    if (b->nseg == 0) return PG_OK;
+    const unsigned long long chunks = b->clear_padded / 16;
+    unsigned long long blocks = (chunks + 255) / 256;
+    const unsigned long long cap = (unsigned long long)b->num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    k_batch_clear<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        b->d_seg_ptr, b->d_seg_bytes, b->d_seg_end, b->nseg, b->clear_padded);
+    return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
 }
 
 pg_status pg_batch_set_launch(pg_batch *b, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t lanes_per_key)

@@ -51,10 +51,15 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 // The fingerprint walk is latency-bound on L2 round trips: full occupancy (8
 // blocks of 256, 32 registers) measured 7 % faster on the region-ordered
 // insert at 2^26 slots despite a few bytes of spill.
+#ifndef PG_FILTER_MIN_BLOCKS
+#define PG_FILTER_MIN_BLOCKS 1
+#endif
 template <int FMT>
 constexpr int min_blocks_of()
 {
-    return FMT == FMT_KV64_FP ? 8 : PG_MIN_BLOCKS;
+    if (FMT == FMT_KV64_FP) return 8;
+    if (FMT == FMT_TAGVAL16 || FMT == FMT_TAGVAL16_SPLIT || FMT == FMT_TAG16) return PG_FILTER_MIN_BLOCKS;
+    return PG_MIN_BLOCKS;
 }
 
 template <int FMT, int B, int G, int S0, bool BK, int OP>

@@ -5,15 +5,19 @@
 // requests into "waves" and keeps up to kMaxWaves waves on the GPU at once:
 // while one wave runs, the next is staged and launched behind it, so requests
 // that arrive while others are on the GPU join the next wave instead of
-// waiting for the queue to drain.  A wave is one pinned staging copy in, one
-// pg_batch_run per kernel class (tables of one format / bucket / scheme
-// share a class), and one copy out, all on the server's stream.
+// waiting for the queue to drain.  A wave is one pinned staging copy in (on
+// the upload stream), one pg_batch_run per kernel class (tables of one format
+// / bucket / scheme share a class), each on its class's own stream, and one
+// copy out (on the download stream), ordered by events: the next wave's upload
+// and the previous wave's download run beside this wave's kernels, and the
+// classes of one wave run beside each other.
 //
-// Ordering: requests on one table complete in submission order, and a wave
-// never mixes conflicting requests on a table (only queries share a table
-// with queries, inserts with inserts, removes with removes), so every result
-// equals what the request returns when the requests are run one at a time in
-// submission order (what the plain path does).
+// Ordering: a class's runs are issued on its one stream in wave order, so
+// requests on one table complete in submission order; and a wave never mixes
+// conflicting requests on a table (only queries share a table with queries,
+// inserts with inserts, removes with removes), so every result equals what the
+// request returns when the requests are run one at a time in submission order
+// (what the plain path does).
 //
 // Tables are admitted against an HBM budget: pg_server_add_table fails with
 // PG_ERR_FULL when the table would not fit, and dropping a table releases its
@@ -37,7 +41,7 @@
 
 namespace {
 
-constexpr int kMaxWaves = 2;
+constexpr int kMaxWaves = 3;
 
 struct request {
     uint64_t id;
@@ -63,6 +67,7 @@ struct table_entry {
 
 struct klass {
     pg_batch *batch = nullptr;
+    cudaStream_t stream = nullptr;  // the class's runs, in wave order
     std::vector<uint32_t> tables;  // server table ids in batch order
     uint32_t vbytes;
     bool dirty = true;  // batch must be rebuilt (tables added / dropped)
@@ -79,7 +84,8 @@ double now_s()
 struct pg_server {
     pg_server_config cfg;
     int device;
-    cudaStream_t stream;
+    cudaStream_t stream;  // uploads
+    cudaStream_t down;    // downloads
     std::mutex mu;
     std::condition_variable cv;
     std::thread worker;
@@ -100,6 +106,8 @@ struct pg_server {
         pg_op_desc *h_ops, *d_ops;
         uint32_t *h_nops, *d_nops;
         uint64_t *h_counts, *d_counts;
+        cudaEvent_t uploaded;  // the wave's inputs are on the device
+        cudaEvent_t ran;       // recorded after each class's run, waited on by the download stream
         cudaEvent_t done;
         bool busy;
     } stages[kMaxWaves];
@@ -123,6 +131,15 @@ bool conflicts(uint32_t a, uint32_t b) { return a != b; }
 // staging buffer of a value width: 8 -> 0, 2 -> 1, 1 -> 2
 int width_index(uint32_t vb) { return vb == 8 ? 0 : vb == 2 ? 1 : 2; }
 constexpr uint32_t kWidths[3] = {8, 2, 1};
+
+// wait for every wave the server has issued (uploads, every class's runs, downloads)
+void sync_all(pg_server *s)
+{
+    cudaStreamSynchronize(s->stream);
+    for (auto &k : s->classes)
+        if (k.stream) cudaStreamSynchronize(k.stream);
+    cudaStreamSynchronize(s->down);
+}
 
 pg_status rebuild(pg_server *s, klass &k)
 {
@@ -235,6 +252,7 @@ struct wave_plan {
     std::vector<uint32_t> slot;     // its table's index in the class batch
     struct run {
         pg_batch *batch;
+        cudaStream_t stream;
         uint32_t first, count, vb;
     };
     std::vector<run> runs;  // one pg_batch_run per kernel class, requests [first, first + count)
@@ -308,7 +326,7 @@ void worker_loop(pg_server *s)
             for (auto &k : s->classes) any_dirty |= k.dirty;
             if (any_dirty) {
                 // a class's table list changed: let in-flight waves finish before its batch is rebuilt
-                cudaStreamSynchronize(s->stream);
+                sync_all(s);
                 for (auto &k : s->classes)
                     if (k.dirty) {
                         pg_status st = rebuild(s, k);
@@ -338,7 +356,8 @@ void worker_loop(pg_server *s)
                 pl.slot[i] = te.slot;
                 ko += pl.reqs[i]->n;
                 if (i == 0 || te.cls != s->tables[pl.reqs[i - 1]->table].cls)
-                    pl.runs.push_back({s->classes[te.cls].batch, (uint32_t)i, 0, s->classes[te.cls].vbytes});
+                    pl.runs.push_back({s->classes[te.cls].batch, s->classes[te.cls].stream, (uint32_t)i, 0,
+                                       s->classes[te.cls].vbytes});
                 pl.runs.back().count++;
             }
             pl.nkeys = ko;
@@ -359,30 +378,36 @@ void worker_loop(pg_server *s)
                 st.h_ops[i] = pg_op_desc{pl.slot[i], r->op, o, r->n};
             }
             copy_all(jobs);
-            // one copy in, one run per class, one copy out
+            // one copy in (upload stream), one run per class (its own stream,
+            // after the upload), one copy out (download stream, after every run)
+            for (size_t ci = 0; ci < pl.runs.size(); ci++) st.h_nops[ci] = pl.runs[ci].count;
             cudaMemcpyAsync(st.d_keys, st.h_keys, ko * 8, cudaMemcpyHostToDevice, s->stream);
             for (int x = 0; x < 3; x++)
                 if (any_in[x])
                     cudaMemcpyAsync(st.d_vin[x], st.h_vin[x], ko * kWidths[x], cudaMemcpyHostToDevice, s->stream);
             cudaMemcpyAsync(st.d_ops, st.h_ops, nr * sizeof(pg_op_desc), cudaMemcpyHostToDevice, s->stream);
+            cudaMemcpyAsync(st.d_nops, st.h_nops, pl.runs.size() * 4, cudaMemcpyHostToDevice, s->stream);
             cudaMemsetAsync(st.d_counts, 0, nr * 8, s->stream);
+            cudaEventRecord(st.uploaded, s->stream);
             pg_status launch_error = PG_OK;
             for (size_t ci = 0; ci < pl.runs.size(); ci++) {
                 const wave_plan::run &rn = pl.runs[ci];
-                st.h_nops[ci] = rn.count;
-                cudaMemcpyAsync(st.d_nops + ci, st.h_nops + ci, 4, cudaMemcpyHostToDevice, s->stream);
+                cudaStreamWaitEvent(rn.stream, st.uploaded, 0);
                 const int x = width_index(rn.vb);
                 pg_status rs = pg_batch_run(rn.batch, st.d_ops + rn.first, st.d_nops + ci, st.d_keys, st.d_vin[x],
                                             st.d_vout[x], st.d_flags, st.d_counts + rn.first,
-                                            reinterpret_cast<pg_stream_t>(s->stream));
+                                            reinterpret_cast<pg_stream_t>(rn.stream));
                 if (rs != PG_OK) launch_error = rs;
+                // the download waits for this run (a wait takes the event's latest record)
+                cudaEventRecord(st.ran, rn.stream);
+                cudaStreamWaitEvent(s->down, st.ran, 0);
             }
-            cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->stream);
+            cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->down);
             for (int x = 0; x < 3; x++)
                 if (any_q[x])
-                    cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->stream);
-            cudaMemcpyAsync(st.h_counts, st.d_counts, nr * 8, cudaMemcpyDeviceToHost, s->stream);
-            cudaEventRecord(st.done, s->stream);
+                    cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->down);
+            cudaMemcpyAsync(st.h_counts, st.d_counts, nr * 8, cudaMemcpyDeviceToHost, s->down);
+            cudaEventRecord(st.done, s->down);
             lk.lock();
             if (launch_error != PG_OK) s->error = launch_error;
             slots[w].busy = true;
@@ -416,6 +441,7 @@ pg_status pg_server_create(const pg_server_config *cfg, pg_server **out)
     s->cfg = *cfg;
     cudaGetDevice(&s->device);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking);
     const uint64_t K = cfg->max_wave_keys, R = cfg->max_wave_requests;
     for (int w = 0; w < kMaxWaves && e == cudaSuccess; w++) {
         auto &st = s->stages[w];
@@ -436,6 +462,8 @@ pg_status pg_server_create(const pg_server_config *cfg, pg_server **out)
         if (e == cudaSuccess) e = cudaMalloc(&st.d_nops, R * 4);
         if (e == cudaSuccess) e = cudaMallocHost(&st.h_counts, R * 8);
         if (e == cudaSuccess) e = cudaMalloc(&st.d_counts, R * 8);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.uploaded, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.ran, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming);
     }
     if (e != cudaSuccess) {
@@ -457,8 +485,10 @@ pg_status pg_server_destroy(pg_server *s)
     }
     s->cv.notify_all();
     if (s->worker.joinable()) s->worker.join();
-    for (auto &k : s->classes)
+    for (auto &k : s->classes) {
         if (k.batch) pg_batch_destroy(k.batch);
+        if (k.stream) cudaStreamDestroy(k.stream);
+    }
     for (auto &te : s->tables)
         if (te.live) pg_table_destroy(te.t);
     for (auto &st : s->stages) {
@@ -478,11 +508,14 @@ pg_status pg_server_destroy(pg_server *s)
         cudaFree(st.d_nops);
         cudaFreeHost(st.h_counts);
         cudaFree(st.d_counts);
+        if (st.uploaded) cudaEventDestroy(st.uploaded);
+        if (st.ran) cudaEventDestroy(st.ran);
         if (st.done) cudaEventDestroy(st.done);
     }
     for (auto &kv : s->done) delete kv.second;
     for (request *r : s->pending) delete r;
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->down) cudaStreamDestroy(s->down);
     delete s;
     return PG_OK;
 }
@@ -519,8 +552,15 @@ pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t
         }
     }
     if (cls == s->classes.size()) {
+        cudaStream_t cs = nullptr;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            pg_table_destroy(t);
+            return PG_ERR_CUDA;
+        }
         s->classes.push_back(klass());
         s->classes.back().vbytes = vb;
+        s->classes.back().stream = cs;
     }
     table_entry te;
     te.t = t;
@@ -550,7 +590,7 @@ pg_status pg_server_drop_table(pg_server *s, uint32_t table_id)
     k.tables.erase(std::remove(k.tables.begin(), k.tables.end(), table_id), k.tables.end());
     k.dirty = true;
     // waves already on the GPU may still use the table
-    cudaStreamSynchronize(s->stream);
+    sync_all(s);
     pg_table_destroy(te.t);
     te.t = nullptr;
     s->bytes_used -= te.bytes;

@@ -6,7 +6,10 @@
 // free_from_array): every thread mallocs one object and writes into it, a
 // bitmap over object offsets catches any object handed out twice, every
 // object is freed, the whole pool is allocated a second time, and a second
-// free of the same object is counted.  Prints one JSON line.
+// free of the same object is counted.  A third pass calls malloc() from three
+// divergent branches of one warp (each branch its own call site, after
+// different amounts of work), the way arbitrary device code may call it.
+// Prints one JSON line.
 #include <cstdio>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -33,6 +36,37 @@ __global__ void allocate_into_array_bits(allocator *a, uint64_t *ptrs, uint64_t 
     if (old & (1ULL << (off % 64))) atomicAdd(c + 2, 1ULL);  // handed out twice
 }
 
+// malloc() from divergent code: the lanes of a warp split three ways by a hash
+// of their index, do different amounts of work, and allocate at three call sites
+__global__ void allocate_divergent(allocator *a, uint64_t *ptrs, uint64_t *bitmap, uint64_t n,
+                                   unsigned long long *c)
+{
+    uint64_t tid = threadIdx.x + (uint64_t)blockIdx.x * blockDim.x;
+    if (tid >= n) return;
+    uint32_t h = (uint32_t)(tid * 2654435761ULL >> 7);
+    void *p;
+    uint32_t x = h;
+    if (h % 3 == 0) {
+        p = a->malloc();
+    } else if (h % 3 == 1) {
+        for (int i = 0; i < (int)(h & 15); ++i) x = x * 1664525u + 1013904223u;
+        p = a->malloc();
+    } else {
+        for (int i = 0; i < 40 + (int)(h & 31); ++i) x = x * 22695477u + 1u;
+        p = a->malloc();
+    }
+    ptrs[tid] = (uint64_t)p;
+    if (!p) {
+        atomicAdd(c + 0, 1ULL);
+        return;
+    }
+    ((uint32_t *)p)[0] = x;
+    uint64_t off = a->get_offset_from_ptr(p);
+    if (off >= a->get_largest_allocation_offset()) atomicAdd(c + 1, 1ULL);
+    unsigned long long old = atomicOr((unsigned long long *)&bitmap[off / 64], 1ULL << (off % 64));
+    if (old & (1ULL << (off % 64))) atomicAdd(c + 2, 1ULL);
+}
+
 __global__ void free_from_array(allocator *a, uint64_t *ptrs, uint64_t n)
 {
     uint64_t tid = threadIdx.x + (uint64_t)blockIdx.x * blockDim.x;
@@ -57,8 +91,8 @@ int main()
     unsigned long long *c;
     cudaMalloc(&ptrs, n * 8);
     cudaMalloc(&bitmap, n / 8);
-    cudaMalloc(&c, 8 * 8);
-    cudaMemset(c, 0, 8 * 8);
+    cudaMalloc(&c, 16 * 8);
+    cudaMemset(c, 0, 16 * 8);
     const unsigned blocks = (unsigned)((n + 255) / 256);
     cudaMemset(bitmap, 0, n / 8);
     allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c);
@@ -70,9 +104,14 @@ int main()
     cudaMemset(bitmap, 0, n / 8);
     allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c + 3);
     cudaDeviceSynchronize();
+    free_from_array<<<blocks, 256>>>(a, ptrs, n);
+    cudaMemset(bitmap, 0, n / 8);
+    allocate_divergent<<<blocks, 256>>>(a, ptrs, bitmap, n, c + 8);
+    cudaDeviceSynchronize();
+    const uint64_t fill_divergent = a->report_fill();
     double_free<<<1, 32>>>(a, ptrs, (uint64_t *)(c + 6));
     cudaError_t e = cudaDeviceSynchronize();
-    unsigned long long h[8];
+    unsigned long long h[16];
     cudaMemcpy(h, c, sizeof(h), cudaMemcpyDeviceToHost);
     allocator::free_on_device(a);
     cudaFree(ptrs);
@@ -80,10 +119,13 @@ int main()
     cudaFree(c);
     printf("{\"allocs\": %llu, \"misses\": %llu, \"out_of_pool\": %llu, \"duplicates\": %llu, "
            "\"misses_2\": %llu, \"out_of_pool_2\": %llu, \"duplicates_2\": %llu, \"double_free_refused\": %llu, "
-           "\"free_slabs_when_full\": %llu, \"free_slabs_after_free\": %llu, \"slabs\": %llu, \"cuda\": %d}\n",
+           "\"free_slabs_when_full\": %llu, \"free_slabs_after_free\": %llu, \"slabs\": %llu, "
+           "\"misses_divergent\": %llu, \"out_of_pool_divergent\": %llu, \"duplicates_divergent\": %llu, "
+           "\"free_slabs_divergent\": %llu, \"cuda\": %d}\n",
            (unsigned long long)n, h[0], h[1], h[2], h[3], h[4], h[5], h[6], (unsigned long long)fill_full,
-           (unsigned long long)fill_empty, (unsigned long long)slabs, (int)e);
+           (unsigned long long)fill_empty, (unsigned long long)slabs, h[8], h[9], h[10],
+           (unsigned long long)fill_divergent, (int)e);
     const bool ok = e == cudaSuccess && !h[0] && !h[1] && !h[2] && !h[3] && !h[4] && !h[5] && h[6] == 1 &&
-                    fill_full == 0 && fill_empty == slabs;
+                    fill_full == 0 && fill_empty == slabs && !h[8] && !h[9] && !h[10] && fill_divergent == 0;
     return ok ? 0 : 1;
 }

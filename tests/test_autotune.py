@@ -35,3 +35,35 @@ def test_tuner_keeps_layout_flags_and_caches_the_best(pg, tmp_path, monkeypatch)
     assert s == at.Shape(1, 256, 8, 8)
     d = json.loads((tmp_path / "tune.json").read_text())
     assert list(d.values())[0]["shape"]["tile"] == 1
+
+
+def test_batch_pick_is_the_fastest_shape_with_few_failures():
+    R, S = at.BatchResult, at.BatchShape
+    res = [R(S(1, 16, 8), 10.0, 0), R(S(1, 8, 8), 5.0, 500), R(S(2, 16, 8), 9.0, 10), R(S(4, 32, 4), 12.0, 0)]
+    # the 5 ms shape fails 500 keys, far more than the fewest (0): not eligible
+    assert at.best_batch(res).shape == S(2, 16, 8)
+
+
+def test_batch_cache_key_separates_size_classes(pg):
+    small = [pg.data_structs.tcf(1 << 12, 64) for _ in range(8)]
+    large = [pg.data_structs.tcf(1 << 20, 1 << 13) for _ in range(8)]
+    many = [pg.data_structs.tcf(1 << 12, 64) for _ in range(1024)]
+    keys = {at.batch_cache_key("B200", c) for c in (small, large, many)}
+    assert len(keys) == 3
+
+
+def test_tuned_batch_shape_caches_the_pick(pg, tmp_path, monkeypatch):
+    monkeypatch.setattr(at, "CACHE", tmp_path / "tune.json")
+    monkeypatch.setattr(torch.cuda, "get_device_name", lambda *a: "B200")
+    calls = []
+
+    def fake_sweep(make, seeds, *a, **grid):
+        calls.append(make(8)[0].levels[0].bucket_size)
+        return [at.BatchResult(at.BatchShape(l, 16, 8), 1.0 + l, 0) for l in (1, 2, 4)]
+
+    monkeypatch.setattr(at, "sweep_batch", fake_sweep)
+    make = lambda b: [pg.data_structs.tcf(1 << 14, 164, bucket=b)]
+    s, res = at.tuned_batch_shape(make, [1], None, None, None, None, None, None)
+    assert s == at.BatchShape(1, 16, 8) and len(res) == 3 and calls == [8]
+    s2, res2 = at.tuned_batch_shape(make, [1], None, None, None, None, None, None)
+    assert s2 == s and res2 is None and calls == [8]

@@ -187,3 +187,51 @@ def test_batch_skips_insert_with_delete_on_other_tables(pg):
     keys = wl.keys_without_sentinels(3, 100)
     f, _, c = _run(pg, b, [keys], pg.PG_OP_INSERT_WITH_DELETE, torch.int64, [wl.values_for(keys, 8, 1)])
     assert not f[0].any() and c[0] == 0 and t.get_fill(0)[0] == 0
+
+
+def test_batch_clear_zeroes_every_table_in_one_launch(pg):
+    """pg_batch_clear leaves every table of the batch as pg_table_clear would:
+    all levels (and fingerprint arrays) zero, nothing found afterwards."""
+    import torch
+    from tests.gpu_util import Driver
+    cfgs = [pg.data_structs.tcf(1 << 12, 64), pg.data_structs.tcf(5000, 50), pg.data_structs.tcf(1 << 14, 164)]
+    tables = [pg.Table(c, 7 + i) for i, c in enumerate(cfgs)]
+    keys = [wl.keys_without_sentinels(600 + i, 2000) for i in range(3)]
+    for t, k in zip(tables, keys):
+        Driver(t).insert(k, wl.values_for(k, 2, 1))
+    assert all(t.get_fill(0)[0] > 0 for t in tables)
+    b = pg.Batch(tables, max_ops=4)
+    b.clear()
+    torch.cuda.synchronize()
+    for t, k in zip(tables, keys):
+        assert t.get_fill(0) == (0, 0) and t.get_fill(1) == (0, 0)
+        assert all(x == 0 for l in range(2) for x in t.dump_level(l))
+        f, _ = Driver(t).query(k)
+        assert not f.any()
+    b.free()
+
+
+def test_batch_sweep_times_every_shape_of_a_small_grid(pg, tmp_path, monkeypatch):
+    import torch
+    from poggers_b200 import autotune as at
+    monkeypatch.setattr(at, "CACHE", tmp_path / "tune.json")
+    sizes = [1 << 12, 3000, 1 << 13]
+    ks = [wl.keys_without_sentinels(700 + i, int(0.9 * n)) for i, n in enumerate(sizes)]
+    qs = [np.concatenate([k[: len(k) // 2], wl.keys_without_sentinels(800 + i, len(k) - len(k) // 2)])
+          for i, k in enumerate(ks)]
+    offs = np.concatenate([[0], np.cumsum([len(k) for k in ks])])
+    ins = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_INSERT, int(offs[i]), len(k)) for i, k in enumerate(ks)])).cuda()
+    qo = torch.from_numpy(pg.pack_ops([(i, pg.PG_OP_QUERY, int(offs[i]), len(k)) for i, k in enumerate(ks)])).cuda()
+    nops = torch.tensor([3], dtype=torch.int32, device="cuda")
+    allk = np.concatenate(ks)
+    dk, dv, dq = to_dev(allk), to_dev((wl.values_for(allk, 2, 3) & np.uint64(0xFFFF)).astype(np.uint16)), \
+        to_dev(np.concatenate(qs))
+
+    def make(bucket):
+        return [pg.data_structs.tcf(n, max(n // 100, 64), bucket=bucket) for n in sizes]
+
+    shape, res = at.tuned_batch_shape(make, [1, 2, 3], ins, qo, nops, dk, dv, dq, lanes=(1, 4), buckets=(8, 16),
+                                      blocks_per_sm=(8,), reps=1)
+    assert {(r.shape.lanes, r.shape.bucket) for r in res} == {(1, 8), (4, 8), (1, 16), (4, 16)}
+    assert all(r.step_ms > 0 for r in res)
+    assert shape in [r.shape for r in res]

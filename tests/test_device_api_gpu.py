@@ -62,3 +62,6 @@ def test_slab_allocator_device_api(drivers):
     assert d["misses"] == 0 and d["duplicates"] == 0 and d["out_of_pool"] == 0
     assert d["misses_2"] == 0 and d["duplicates_2"] == 0 and d["double_free_refused"] == 1
     assert d["free_slabs_when_full"] == 0 and d["free_slabs_after_free"] == d["slabs"] == d["allocs"] // 4096
+    # malloc() called from divergent branches of a warp: the whole pool, each object once
+    assert d["misses_divergent"] == 0 and d["duplicates_divergent"] == 0 and d["out_of_pool_divergent"] == 0
+    assert d["free_slabs_divergent"] == 0

@@ -214,13 +214,23 @@ def test_full_size_ht_workload_matches_reference(pg, full_size_ht_oracle, layout
     assert res["n_remove_exceptions"] == 0
     assert res["n_requery_exceptions"] == 0
     # the reference's own parallel build failed 125 of these inserts, the
-    # sequential oracle 119; which ones fail depends on the order of the CASes,
-    # so the count is a random variable: within three standard deviations
-    # (Poisson) of the reference's
+    # sequential oracle 119.  Which ones fail depends on the order in which the
+    # claims land, so the count is a random variable: the benchmarked region
+    # order stays within three standard deviations (Poisson) of the
+    # reference's.  In batch order a key that walks more full buckets claims
+    # its slot later than its neighbours and so meets a fuller table; over four
+    # key seeds that order failed 1.05-1.30x the sequential oracle's count on
+    # the same keys (152-188 against 119-159), with every occupied slot
+    # accounted for, so it gets that margin.
     stats = _load_stats()
     ref_failed = len(stats["ht"]["insert_failed"]) if stats is not None else 125
     nfail = int((~ok).sum())
-    assert nfail <= ref_failed + 3 * ref_failed ** 0.5, f"{nfail} insert failures, reference {ref_failed}"
+    bound = ref_failed + 3 * ref_failed ** 0.5 if insert_order == "region" else 1.5 * ref_failed
+    assert nfail <= bound, f"{nfail} insert failures, reference {ref_failed}"
+    # no capacity lost: every occupied slot holds a placed key (removed keys
+    # leave tombstones, which stay occupied)
+    occ, tomb = t.get_fill(0)
+    assert occ == n - nfail and tomb == int(r.sum()), "occupied slots differ from the inserts that succeeded"
     # bit-exact against the oracle on every key both runs placed
     both = ok & o["ok"]
     qboth = np.concatenate([both[:half], np.ones(len(qkeys) - half, dtype=bool)])
