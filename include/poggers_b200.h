@@ -434,6 +434,48 @@ pg_status pg_slab_set_bulk_free(pg_slab_set *s, void *const *d_ptrs, uint64_t n,
                                 pg_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Pinned slab pool: the reference's own slab policy, whose NULL returns,
+ * report_fill and free counters equal the reference's on the same calls.
+ * Every SM pins a primary slab and extra_blocks backups when the pool is
+ * created; a malloc claims a whole 64-object word of the primary and keeps
+ * the objects it does not use in its SM's cache; when the primary has no whole
+ * word left a backup takes its place and the pool refills the backup's place.
+ * So a malloc can return NULL while other SMs' slabs still hold free objects,
+ * and report_fill counts only the slabs in the pool.  (pg_slab_create's pool
+ * returns NULL only when the whole pool is full.)  The template API's
+ * one_size_slab_allocator<extra_blocks> is built on this pool.
+ *   pg_pslab_create       <- one_size_slab_allocator<E>::generate_on_device  slab_one_size.cuh:84-141
+ *                            (pins: smid_pinned_container::generate_on_device offset_slab.cuh:1838-1873)
+ *   pg_pslab_bulk_malloc  <- malloc() one thread per allocation         slab_one_size.cuh:186-288
+ *   pg_pslab_bulk_free    <- free / free_count_misses                   slab_one_size.cuh:428-506
+ *   pg_pslab_report       <- report_fill / report_max                   slab_one_size.cuh:628-654
+ * --------------------------------------------------------------------------- */
+typedef struct pg_pslab pg_pslab;
+/* Pool of ceil(num_allocs / 4096) slabs; extra_blocks backups per SM (< 63).
+ * Synchronous; SM ids are those below the device's %nsmid. */
+pg_status pg_pslab_create(uint64_t num_allocs, uint64_t object_bytes, uint32_t extra_blocks, pg_pslab **out);
+pg_status pg_pslab_destroy(pg_pslab *a);
+/* Device descriptor for device callers of include/poggers_b200/slab_pinned.cuh;
+ * `bytes` must equal sizeof(pg::pslab_desc). */
+pg_status pg_pslab_desc(const pg_pslab *a, void *out_desc, uint64_t bytes);
+/* Synchronous report: slabs in the pool (report_fill), slabs (report_max),
+ * SM ids with pins, double frees seen. */
+pg_status pg_pslab_report(const pg_pslab *a, uint64_t *pool_slabs, uint64_t *max_slabs, uint64_t *sm_ids,
+                          uint64_t *double_frees);
+/* d_ptrs[i] = an object or NULL, one malloc() per thread; d_fail_count (optional) += NULLs. */
+pg_status pg_pslab_bulk_malloc(pg_pslab *a, uint64_t n, void **d_ptrs, uint64_t *d_fail_count, pg_stream_t stream);
+/* The serial launch shape: one warp makes `rounds` malloc() calls of `group`
+ * lanes (1..32) each, in order; d_ptrs[k * group + lane]. */
+pg_status pg_pslab_serial_malloc(pg_pslab *a, uint32_t rounds, uint32_t group, void **d_ptrs, uint64_t *d_fail_count,
+                                 pg_stream_t stream);
+/* Free d_ptrs[0..n) (NULL entries skipped), one thread per pointer, or in
+ * order by one thread when `serial`; d_counts[0..3] += frees refused (double
+ * or foreign), frees done, slabs returned to the pool (free_count_misses'
+ * misses[0]), slabs emptied while pinned (misses[1]). */
+pg_status pg_pslab_bulk_free(pg_pslab *a, void *const *d_ptrs, uint64_t n, uint64_t *d_counts, int serial,
+                             pg_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Diagnostics (no counterpart in the reference): the GPU's random-access
  * ceilings, which bound the filters' kernels (one or two 32-byte sectors at
  * random addresses per key, and an atomic claim on a sector just read).

@@ -149,6 +149,22 @@ uint64_t pgo_btable_bulk(pgo_btable *t, int op, const uint64_t *keys, const uint
                          uint64_t *out, uint8_t *ok, uint8_t *found);
 uint64_t pgo_btable_count_fill(const pgo_btable *t, int level);
 
+/* restatement of the reference's one_size_slab_allocator<E> (poggers_oracle_slabref.c):
+ * per-SM pinned slabs, whole-word claims with a per-SM cache, pivot and pool */
+typedef struct pgo_rslab pgo_rslab;
+enum { PGO_RSLAB_REFUSED = 0, PGO_RSLAB_FREED = 1, PGO_RSLAB_RETURNED = 2, PGO_RSLAB_EMPTIED_PINNED = 3 };
+pgo_rslab *pgo_rslab_create(uint64_t num_allocs, int sms, int extra_blocks, uint64_t seed);
+void pgo_rslab_destroy(pgo_rslab *a);
+uint64_t pgo_rslab_report_fill(const pgo_rslab *a);
+uint64_t pgo_rslab_report_max(const pgo_rslab *a);
+uint64_t pgo_rslab_short_pins(const pgo_rslab *a);
+uint64_t pgo_rslab_lost_words(const pgo_rslab *a);
+/* one malloc() call by `group` threads of one warp (1..32) on SM `sm`, served
+ * together; out[i] = object offset or ~0; returns the NULL count */
+uint64_t pgo_rslab_malloc(pgo_rslab *a, int sm, int group, uint64_t *out);
+/* one free(); returns PGO_RSLAB_* */
+int pgo_rslab_free(pgo_rslab *a, uint64_t offset);
+
 /* splitmix64 key stream: key i = mix(seed + (i+1) * 0x9E3779B97F4A7C15) */
 void pgo_splitmix64_fill(uint64_t seed, uint64_t start, uint64_t n, uint64_t *out);
 

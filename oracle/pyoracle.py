@@ -121,6 +121,16 @@ def lib():
         L.pgo_btable_bulk.argtypes = [C.c_void_p, C.c_int, U64P, U64P, C.c_uint64, U64P, U8P, U8P]
         L.pgo_btable_count_fill.restype = C.c_uint64
         L.pgo_btable_count_fill.argtypes = [C.c_void_p, C.c_int]
+        L.pgo_rslab_create.restype = C.c_void_p
+        L.pgo_rslab_create.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_uint64]
+        L.pgo_rslab_destroy.argtypes = [C.c_void_p]
+        for f in ("pgo_rslab_report_fill", "pgo_rslab_report_max", "pgo_rslab_short_pins", "pgo_rslab_lost_words"):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_void_p]
+        L.pgo_rslab_malloc.restype = C.c_uint64
+        L.pgo_rslab_malloc.argtypes = [C.c_void_p, C.c_int, C.c_int, U64P]
+        L.pgo_rslab_free.restype = C.c_int
+        L.pgo_rslab_free.argtypes = [C.c_void_p, C.c_uint64]
         _lib = L
     return _lib
 
@@ -307,3 +317,44 @@ class OracleBucketed:
 
     def count_fill(self, level: int) -> int:
         return lib().pgo_btable_count_fill(self.h, level)
+
+
+RSLAB_REFUSED, RSLAB_FREED, RSLAB_RETURNED, RSLAB_EMPTIED_PINNED = range(4)
+
+
+class RefSlab:
+    """Sequential restatement of the reference's one_size_slab_allocator<E>
+    (per-SM pinned slabs, whole-word claims with a per-SM cache, pivot, pool)."""
+
+    def __init__(self, num_allocs: int, sms: int, extra_blocks: int, seed: int = 1):
+        self.h = lib().pgo_rslab_create(num_allocs, sms, extra_blocks, seed)
+        if not self.h:
+            raise ValueError("invalid slab configuration")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pgo_rslab_destroy(self.h)
+            self.h = None
+
+    def report_fill(self) -> int:
+        return lib().pgo_rslab_report_fill(self.h)
+
+    def report_max(self) -> int:
+        return lib().pgo_rslab_report_max(self.h)
+
+    @property
+    def short_pins(self) -> int:
+        return lib().pgo_rslab_short_pins(self.h)
+
+    @property
+    def lost_words(self) -> int:
+        return lib().pgo_rslab_lost_words(self.h)
+
+    def malloc(self, sm: int, group: int):
+        """One malloc() by `group` lanes of a warp on SM `sm`: (offsets or ~0, NULL count)."""
+        out = np.zeros(32, dtype=np.uint64)
+        nulls = lib().pgo_rslab_malloc(self.h, sm, group, _p64(out))
+        return out[:group], int(nulls)
+
+    def free(self, offset: int) -> int:
+        return lib().pgo_rslab_free(self.h, int(offset))

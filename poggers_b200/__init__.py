@@ -92,6 +92,8 @@ EXPORTED = (
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
     "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
     "pg_batch_clear",
+    "pg_pslab_create", "pg_pslab_destroy", "pg_pslab_desc", "pg_pslab_report", "pg_pslab_bulk_malloc",
+    "pg_pslab_serial_malloc", "pg_pslab_bulk_free",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
     "pg_diag_random_access",
@@ -188,6 +190,20 @@ def lib() -> C.CDLL:
     L.pg_batch_set_launch.argtypes = [V, U32, U32, U32]
     L.pg_batch_run.restype = C.c_int
     L.pg_batch_run.argtypes = [V, P, P, P, P, P, P, P, P]
+    L.pg_pslab_create.restype = C.c_int
+    L.pg_pslab_create.argtypes = [U64, U64, U32, C.POINTER(V)]
+    L.pg_pslab_destroy.restype = C.c_int
+    L.pg_pslab_destroy.argtypes = [V]
+    L.pg_pslab_desc.restype = C.c_int
+    L.pg_pslab_desc.argtypes = [V, P, U64]
+    L.pg_pslab_report.restype = C.c_int
+    L.pg_pslab_report.argtypes = [V, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]
+    L.pg_pslab_bulk_malloc.restype = C.c_int
+    L.pg_pslab_bulk_malloc.argtypes = [V, U64, P, P, P]
+    L.pg_pslab_serial_malloc.restype = C.c_int
+    L.pg_pslab_serial_malloc.argtypes = [V, U32, U32, P, P, P]
+    L.pg_pslab_bulk_free.restype = C.c_int
+    L.pg_pslab_bulk_free.argtypes = [V, P, U64, P, C.c_int, P]
     L.pg_batch_clear.restype = C.c_int
     L.pg_batch_clear.argtypes = [V, P]
     L.pg_batch_run_static.restype = C.c_int
@@ -592,6 +608,48 @@ class allocators:
 
         def report_max(self) -> int:
             return self.report()["max_slabs"]
+
+    class pinned_pool:
+        """The reference's slab policy (pg_pslab_*): primary + extra_blocks
+        backups pinned per SM, whole-word claims with a per-SM cache, pivot
+        and pool.  The template API's one_size_slab_allocator is built on it."""
+
+        def __init__(self, num_allocs: int, object_bytes: int, extra_blocks: int):
+            h = C.c_void_p()
+            _check(lib().pg_pslab_create(num_allocs, object_bytes, extra_blocks, C.byref(h)), "pg_pslab_create")
+            self._h = h
+
+        def free_on_device(self) -> None:
+            if getattr(self, "_h", None):
+                lib().pg_pslab_destroy(self._h)
+                self._h = None
+
+        def __del__(self):
+            try:
+                self.free_on_device()
+            except Exception:
+                pass
+
+        def report(self) -> dict:
+            v = [C.c_uint64() for _ in range(4)]
+            _check(lib().pg_pslab_report(self._h, *[C.byref(x) for x in v]), "pg_pslab_report")
+            return {"report_fill": v[0].value, "report_max": v[1].value, "sm_ids": v[2].value,
+                    "double_frees": v[3].value}
+
+        def bulk_malloc(self, ptrs_out, fail_count=None, stream=None, n: int | None = None) -> None:
+            n = ptrs_out.numel() if n is None else n
+            _check(lib().pg_pslab_bulk_malloc(self._h, n, _ptr(ptrs_out), _ptr(fail_count), _stream(stream)),
+                   "pg_pslab_bulk_malloc")
+
+        def serial_malloc(self, rounds: int, group: int, ptrs_out, fail_count=None, stream=None) -> None:
+            _check(lib().pg_pslab_serial_malloc(self._h, rounds, group, _ptr(ptrs_out), _ptr(fail_count),
+                                                _stream(stream)), "pg_pslab_serial_malloc")
+
+        def bulk_free(self, ptrs, counts, serial: bool = False, stream=None, n: int | None = None) -> None:
+            """counts (4 x int64, added to): refused, freed, returned to the pool, emptied while pinned."""
+            n = ptrs.numel() if n is None else n
+            _check(lib().pg_pslab_bulk_free(self._h, _ptr(ptrs), n, _ptr(counts), int(serial), _stream(stream)),
+                   "pg_pslab_bulk_free")
 
     class size_class_set:
         """One pool per size class; each request goes to the smallest class that fits."""

@@ -51,8 +51,12 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 // The fingerprint walk is latency-bound on L2 round trips: full occupancy (8
 // blocks of 256, 32 registers) measured 7 % faster on the region-ordered
 // insert at 2^26 slots despite a few bytes of spill.
+// The filters' kernels (16-bit tags) are bound by random sector reads and
+// need many keys in flight: held to 6 resident blocks of 256 (40 registers,
+// a few spilled words) they ran 1.2-1.4x faster than at their natural 93-103
+// registers (2 blocks).
 #ifndef PG_FILTER_MIN_BLOCKS
-#define PG_FILTER_MIN_BLOCKS 1
+#define PG_FILTER_MIN_BLOCKS 6
 #endif
 template <int FMT>
 constexpr int min_blocks_of()

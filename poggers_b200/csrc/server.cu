@@ -535,7 +535,8 @@ pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t
         if (L.bucket_size == 0 || L.nslots == 0) return PG_ERR_INVALID;
         const uint64_t nb = (L.nslots - 1) / L.bucket_size + 1;
         need += nb * L.bucket_size * (kb + vb);
-        if (l == 0 && (cfg->flags & PG_TABLE_FINGERPRINTS)) need += nb * L.bucket_size;
+        if (l == 0 && (cfg->flags & PG_TABLE_FINGERPRINTS))
+            need += (nb * L.bucket_size + 255) / 256 * 256 + nb * 4;  // fingerprint bytes, then bucket counters
     }
     std::lock_guard<std::mutex> g(s->mu);
     if (s->bytes_used + need > s->cfg.hbm_budget_bytes) return PG_ERR_FULL;

@@ -224,13 +224,22 @@ __global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, u
     }
 }
 
-// fingerprint bytes recomputed from the slots (after a level is loaded)
-__global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, unsigned char *fp, uint64_t nslots,
-                                                    uint64_t seed)
+// fingerprint bytes and bucket counters recomputed from the slots (after a
+// level is loaded): a bucket's counter is its filled prefix, the index of its
+// first empty slot
+__global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, unsigned char *fp, unsigned int *cnt,
+                                                    uint64_t nbuckets, uint32_t B, uint64_t seed)
 {
-    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t key = *reinterpret_cast<const unsigned long long *>(base + 16 * s);
-        fp[s] = fp_of(key, murmur64a_u64(key, seed));
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbuckets;
+         b += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t filled = B;
+        for (uint32_t j = 0; j < B; ++j) {
+            const uint64_t s = b * B + j;
+            const uint64_t key = *reinterpret_cast<const unsigned long long *>(base + 16 * s);
+            fp[s] = fp_of(key, murmur64a_u64(key, seed));
+            if (key == 0 && filled == B) filled = j;
+        }
+        cnt[b] = filled;
     }
 }
 
@@ -330,8 +339,11 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
         }
         D.base = static_cast<unsigned char *>(t->mem[l]);
         D.fp = nullptr;
+        D.cnt = nullptr;
         if (l == 0 && fingerprinted(cfg)) {
-            t->fp_bytes = nb * L.bucket_size;
+            // one allocation: the fingerprint bytes, then a 4-byte counter per bucket
+            const uint64_t fp_span = (nb * L.bucket_size + 255) / 256 * 256;
+            t->fp_bytes = fp_span + nb * 4;
             e = cudaMalloc(&t->fp, t->fp_bytes);
             if (e == cudaSuccess) e = cudaMemset(t->fp, 0, t->fp_bytes);
             if (e != cudaSuccess) {
@@ -340,7 +352,8 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
                 return cuda_status(e);
             }
             D.fp = static_cast<unsigned char *>(t->fp);
-            D.fp_resident = t->fp_bytes <= kFpResidentBytes;
+            D.cnt = reinterpret_cast<unsigned int *>(D.fp + fp_span);
+            D.fp_resident = nb * L.bucket_size <= kFpResidentBytes;
         }
         s = s * s;  // recursive table gets seed*seed (base_table.cuh:124)
     }
@@ -550,7 +563,7 @@ pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src,
     if (!split_layout(&t->cfg)) {
         cudaError_t e = cudaMemcpy(t->mem[level], host_src, t->bytes[level], cudaMemcpyHostToDevice);
         if (e == cudaSuccess && level == 0 && t->fp) {
-            k_rebuild_fp<<<1184, 256>>>(D.base, D.fp, nslots, D.seed);
+            k_rebuild_fp<<<1184, 256>>>(D.base, D.fp, D.cnt, D.nbmod.d, D.bucket_size, D.seed);
             e = cudaDeviceSynchronize();
         }
         return cuda_status(e);

@@ -3,10 +3,12 @@
 //
 // Follows the reference's own drivers (tests/src/slab_one_size_tests.cu:
 // allocate_into_array, the duplicate check of allocate_into_array_bits, and
-// free_from_array): every thread mallocs one object and writes into it, a
-// bitmap over object offsets catches any object handed out twice, every
-// object is freed, the whole pool is allocated a second time, and a second
-// free of the same object is counted.  A third pass calls malloc() from three
+// free_from_array), on a pool provisioned as that test provisions it: every
+// thread mallocs one object and writes into it, a bitmap over object offsets
+// catches any object handed out twice, every object is freed with
+// free_count_misses (slabs returned to the pool / emptied while pinned), the
+// objects are allocated a second time, and a second free of one object is
+// refused.  A third pass calls malloc() from three
 // divergent branches of one warp (each branch its own call site, after
 // different amounts of work), the way arbitrary device code may call it.
 // Prints one JSON line.
@@ -75,57 +77,74 @@ __global__ void free_from_array(allocator *a, uint64_t *ptrs, uint64_t n)
     if (p) a->free(p);
 }
 
+// free everything, counting with free_count_misses: misses[0] slabs returned
+// to the pool, misses[1] slabs emptied while pinned
+__global__ void free_from_array_counted(allocator *a, uint64_t *ptrs, uint64_t n, uint64_t *misses)
+{
+    uint64_t tid = threadIdx.x + (uint64_t)blockIdx.x * blockDim.x;
+    if (tid >= n) return;
+    void *p = (void *)ptrs[tid];
+    if (p) a->free_count_misses(p, misses);
+}
+
+// the second free of one object is refused and counted by neither counter
 __global__ void double_free(allocator *a, uint64_t *ptrs, uint64_t *misses)
 {
     if (threadIdx.x + blockIdx.x * blockDim.x != 0) return;
     void *p = (void *)ptrs[0];
     a->free_count_misses(p, misses);
-    a->free_count_misses(p, misses);  // the second one is refused
+    a->free_count_misses(p, misses);
 }
 
 int main()
 {
-    const uint64_t n = 1ULL << 20;  // 256 slabs of 4096, exactly full
-    allocator *a = allocator::generate_on_device(n, 16);
+    // provisioned as the reference's own test (slab_one_size_tests.cu:226):
+    // 15M objects beyond the ones allocated, for the slabs pinned to SMs
+    const uint64_t n = 1ULL << 20;
+    const uint64_t total = 15000000ULL + n + 4096;
+    allocator *a = allocator::generate_on_device(total, 16);
+    const uint64_t slabs = a->report_max(), fill_initial = a->report_fill(), sms = a->report_pinned_sms();
     uint64_t *ptrs, *bitmap;
     unsigned long long *c;
     cudaMalloc(&ptrs, n * 8);
-    cudaMalloc(&bitmap, n / 8);
+    cudaMalloc(&bitmap, (slabs * 4096) / 8);
     cudaMalloc(&c, 16 * 8);
     cudaMemset(c, 0, 16 * 8);
     const unsigned blocks = (unsigned)((n + 255) / 256);
-    cudaMemset(bitmap, 0, n / 8);
+    cudaMemset(bitmap, 0, (slabs * 4096) / 8);
     allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c);
     cudaDeviceSynchronize();
-    const uint64_t fill_full = a->report_fill(), slabs = a->report_max();
-    free_from_array<<<blocks, 256>>>(a, ptrs, n);
+    const uint64_t fill_full = a->report_fill();
+    free_from_array_counted<<<blocks, 256>>>(a, ptrs, n, (uint64_t *)(c + 11));
     cudaDeviceSynchronize();
     const uint64_t fill_empty = a->report_fill();
-    cudaMemset(bitmap, 0, n / 8);
+    cudaMemset(bitmap, 0, (slabs * 4096) / 8);
     allocate_into_array_bits<<<blocks, 256>>>(a, ptrs, bitmap, n, c + 3);
     cudaDeviceSynchronize();
     free_from_array<<<blocks, 256>>>(a, ptrs, n);
-    cudaMemset(bitmap, 0, n / 8);
+    cudaMemset(bitmap, 0, (slabs * 4096) / 8);
     allocate_divergent<<<blocks, 256>>>(a, ptrs, bitmap, n, c + 8);
     cudaDeviceSynchronize();
-    const uint64_t fill_divergent = a->report_fill();
     double_free<<<1, 32>>>(a, ptrs, (uint64_t *)(c + 6));
     cudaError_t e = cudaDeviceSynchronize();
+    uint64_t pool = 0, ms = 0, ids = 0, doubles = 0;
+    pg_pslab_report(allocator::host_handle(a), &pool, &ms, &ids, &doubles);
     unsigned long long h[16];
     cudaMemcpy(h, c, sizeof(h), cudaMemcpyDeviceToHost);
     allocator::free_on_device(a);
     cudaFree(ptrs);
     cudaFree(bitmap);
     cudaFree(c);
-    printf("{\"allocs\": %llu, \"misses\": %llu, \"out_of_pool\": %llu, \"duplicates\": %llu, "
-           "\"misses_2\": %llu, \"out_of_pool_2\": %llu, \"duplicates_2\": %llu, \"double_free_refused\": %llu, "
-           "\"free_slabs_when_full\": %llu, \"free_slabs_after_free\": %llu, \"slabs\": %llu, "
-           "\"misses_divergent\": %llu, \"out_of_pool_divergent\": %llu, \"duplicates_divergent\": %llu, "
-           "\"free_slabs_divergent\": %llu, \"cuda\": %d}\n",
-           (unsigned long long)n, h[0], h[1], h[2], h[3], h[4], h[5], h[6], (unsigned long long)fill_full,
-           (unsigned long long)fill_empty, (unsigned long long)slabs, h[8], h[9], h[10],
-           (unsigned long long)fill_divergent, (int)e);
-    const bool ok = e == cudaSuccess && !h[0] && !h[1] && !h[2] && !h[3] && !h[4] && !h[5] && h[6] == 1 &&
-                    fill_full == 0 && fill_empty == slabs && !h[8] && !h[9] && !h[10] && fill_divergent == 0;
+    printf("{\"allocs\": %llu, \"slabs\": %llu, \"sm_ids\": %llu, \"fill_initial\": %llu, \"misses\": %llu, "
+           "\"out_of_pool\": %llu, \"duplicates\": %llu, \"fill_full\": %llu, \"returned\": %llu, "
+           "\"emptied_pinned\": %llu, \"fill_empty\": %llu, \"misses_2\": %llu, \"out_of_pool_2\": %llu, "
+           "\"duplicates_2\": %llu, \"misses_divergent\": %llu, \"out_of_pool_divergent\": %llu, "
+           "\"duplicates_divergent\": %llu, \"double_free_counted\": %llu, \"double_free_seen\": %llu, "
+           "\"cuda\": %d}\n",
+           (unsigned long long)n, (unsigned long long)slabs, (unsigned long long)sms, (unsigned long long)fill_initial,
+           h[0], h[1], h[2], (unsigned long long)fill_full, h[11], h[12], (unsigned long long)fill_empty, h[3], h[4],
+           h[5], h[8], h[9], h[10], h[6] + h[7], (unsigned long long)doubles, (int)e);
+    const bool ok = e == cudaSuccess && !h[0] && !h[1] && !h[2] && !h[3] && !h[4] && !h[5] && !h[8] && !h[9] &&
+                    !h[10] && h[6] + h[7] == 0 && doubles == 1;
     return ok ? 0 : 1;
 }

@@ -239,3 +239,88 @@ def test_bucketed_oracle_sawtooth_keeps_its_fill(oracle, bits):
         live[:half], vals[:half] = fresh, fv
         # a query misses only where a remove took a same-tag slot of another key
         assert (~f).sum() <= (20 if bits == 16 else 400), (rnd, int((~f).sum()))
+
+
+# ---- the reference's slab allocator, restated (oracle/poggers_oracle_slabref.c)
+# Known answers derived from the reference's code paths (slab_one_size.cuh:186-288,
+# offset_slab.cuh:330-675, 1466-1780).
+NULL = (1 << 64) - 1
+
+
+def _fill_groups(a, sm, ngroups, group=32):
+    got, nulls = [], 0
+    for _ in range(ngroups):
+        o, n = a.malloc(sm, group)
+        got += [int(x) for x in o if x != NULL]
+        nulls += n
+    return got, nulls
+
+
+def test_refslab_pins_at_creation_and_counts_the_pool(oracle):
+    a = oracle.RefSlab(300 * 4096, sms=148, extra_blocks=1)
+    assert a.report_max() == 300 and a.report_fill() == 300 - 148 * 2 and a.short_pins == 0
+    # the reference's own test flow is over-provisioned: 15M + n + 4096 objects, 16 pins per SM
+    b = oracle.RefSlab(15000000 + (1 << 20) + 4096, sms=148, extra_blocks=15)
+    assert b.report_fill() == b.report_max() - 148 * 16
+    got, nulls = [], 0
+    for g in range((1 << 20) // 32):
+        o, n = b.malloc(g % 148, 32)
+        got += [int(x) for x in o]
+        nulls += n
+    assert nulls == 0 and len(set(got)) == 1 << 20 and max(got) < b.report_max() * 4096
+
+
+def test_refslab_without_backups_never_uses_the_pool(oracle):
+    # E = 0: one pinned slab; its 4096 objects, then every malloc fails
+    # (the pivot finds no backup and leaves the primary place busy)
+    a = oracle.RefSlab(2 * 4096, sms=1, extra_blocks=0)
+    got, nulls = _fill_groups(a, 0, 128)
+    assert nulls == 0 and len(set(got)) == 4096 and all(x // 4096 == got[0] // 4096 for x in got)
+    o, n = a.malloc(0, 32)
+    assert n == 32 and a.report_fill() == 1
+    o, n = a.malloc(0, 1)
+    assert n == 1
+
+
+def test_refslab_pivot_refills_from_the_pool_then_returns_null(oracle):
+    # E = 1, three slabs: A (primary) and B (backup) pinned, C in the pool
+    a = oracle.RefSlab(3 * 4096, sms=1, extra_blocks=1)
+    assert a.report_fill() == 1
+    got, nulls = _fill_groups(a, 0, 128)          # A: 4096 objects
+    assert nulls == 0 and a.report_fill() == 1
+    o, n = a.malloc(0, 32)                          # A has no whole word: B becomes primary, C refills
+    assert n == 0 and a.report_fill() == 0
+    got += [int(x) for x in o]
+    got2, nulls = _fill_groups(a, 0, 127)           # the rest of B
+    assert nulls == 0
+    o, n = a.malloc(0, 32)                          # B exhausted, C primary, the pool is empty:
+    assert n == 1                                   # the pivot's winner returns NULL, the others retry on C
+    got2 += [int(x) for x in o if x != NULL]
+    more, nulls = _fill_groups(a, 0, 140)           # the rest of C, then NULL: no backup is left
+    every = got + got2 + more
+    assert len(every) == 3 * 4096 and len(set(every)) == len(every)
+    o, n = a.malloc(0, 32)
+    assert n == 32
+
+
+def test_refslab_free_returns_only_empty_unpinned_slabs(oracle):
+    a = oracle.RefSlab(3 * 4096, sms=1, extra_blocks=1)
+    first, _ = _fill_groups(a, 0, 128)              # slab A full
+    a.malloc(0, 32)                                 # A unpinned, B primary, C taken: pool empty
+    assert a.report_fill() == 0
+    codes = [a.free(x) for x in first]
+    assert codes.count(oracle.RSLAB_RETURNED) == 1 and codes[-1] == oracle.RSLAB_RETURNED
+    assert codes.count(oracle.RSLAB_REFUSED) == 0 and a.report_fill() == 1
+    assert a.free(first[0]) == oracle.RSLAB_REFUSED  # a double free changes nothing
+    assert a.report_fill() == 1
+    # a pinned slab emptied by frees stays out of the pool; bits of a claimed
+    # word still in the SM's cache keep the slab from being empty
+    b = oracle.RefSlab(2 * 4096, sms=1, extra_blocks=0)
+    got, _ = _fill_groups(b, 0, 3)                  # words 1 and 2 claimed; 32 bits of word 2 cached
+    codes = [b.free(x) for x in got]
+    assert codes.count(oracle.RSLAB_EMPTIED_PINNED) == 0 and codes.count(oracle.RSLAB_RETURNED) == 0
+    c = oracle.RefSlab(2 * 4096, sms=1, extra_blocks=0)
+    got, _ = _fill_groups(c, 0, 4)                  # the cache drained: both words handed out
+    codes = [c.free(x) for x in got]
+    assert codes.count(oracle.RSLAB_EMPTIED_PINNED) == 1 and codes[-1] == oracle.RSLAB_EMPTIED_PINNED
+    assert c.report_fill() == 1
