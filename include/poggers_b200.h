@@ -369,6 +369,17 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
  * seconds from submit to completion), or PG_ERR_TIMEOUT if it is still
  * running and wait == 0.  A request is collected once. */
 pg_status pg_server_poll(pg_server *s, uint64_t request_id, int wait, uint64_t *count, double *latency_s);
+/* Slab size-class sets served by the loop (as pg_slab_set_create; their pools
+ * count against the HBM budget, PG_ERR_FULL when they would not fit).
+ * PG_OP_MALLOC requests take n object sizes (uint32_t) and return n object
+ * pointers (NULL where none was left; count = NULLs); PG_OP_FREE requests take
+ * n pointers (count = refused frees).  Requests on one set complete in
+ * submission order, and a wave never mixes mallocs and frees of one set. */
+enum { PG_OP_MALLOC = 4, PG_OP_FREE = 5 };
+pg_status pg_server_add_slab_set(pg_server *s, uint32_t nclasses, const uint64_t *class_bytes,
+                                 const uint64_t *num_allocs, uint32_t *set_id);
+pg_status pg_server_submit_slab(pg_server *s, uint32_t set_id, uint32_t op, const void *h_in, uint64_t n,
+                                uint64_t *h_ptrs_out, uint64_t *request_id);
 pg_status pg_server_stats(pg_server *s, uint64_t *waves, uint64_t *keys);
 
 /* ---------------------------------------------------------------------------

@@ -70,11 +70,6 @@ constexpr int kTwoChoiceMaxProbes = 4;
 #endif
 // read a two-choice key's second bucket together with its first (see insert_two_choice)
 constexpr bool kTwoChoicePrefetch = PG_TWO_CHOICE_PREFETCH != 0;
-#ifndef PG_FP_CLAIM_COUNTER
-#define PG_FP_CLAIM_COUNTER 1
-#endif
-// fingerprinted levels claim slots by a per-bucket counter (level_ops_fp::claim_counter)
-constexpr bool kFpClaimCounter = PG_FP_CLAIM_COUNTER != 0;
 
 struct level_desc {
     unsigned char *base;   // bucket array
@@ -84,7 +79,6 @@ struct level_desc {
     uint32_t bucket_bytes;
     uint32_t fp_resident;  // 1 when the fingerprint array fits in L2 and is kept there (evict-last loads)
     unsigned char *fp;     // FMT_KV64_FP: one fingerprint byte per slot, else null
-    unsigned int *cnt;     // FMT_KV64_FP: per bucket, the slots taken (its filled prefix), else null
 };
 
 struct table_desc {
@@ -926,37 +920,6 @@ struct level_ops_fp {
             return -1;
         }
     }
-    // Claim by counter: a bucket's filled slots are a prefix (an insert takes
-    // the first empty slot, a remove leaves a tombstone), so its counter of
-    // slots taken is the index of its first empty slot, and one atomicAdd
-    // returns the slot to fill -- one L2 round trip instead of a fingerprint
-    // load and a CAS.  A full bucket's add is undone (an add whose result is
-    // unused), so a counter never exceeds B plus the claims in flight.  The
-    // fingerprint byte is written after the claim; fingerprints and counters
-    // agree again at the end of the launch (queries, removes and inserts of
-    // one table run in separate launches, or in one batch whose order is not
-    // the caller's to observe).
-    __device__ __forceinline__ static int claim_counter(const level_desc &L, uint64_t b)
-    {
-        unsigned int *c = L.cnt + b;
-        const unsigned int old = atomicAdd(c, 1u);
-        if (old < (unsigned int)B) return (int)old;
-        atomicSub(c, 1u);
-        return -1;
-    }
-    // the key 0 (the empty sentinel) takes nothing: the bucket's first empty slot, unclaimed
-    __device__ __forceinline__ static int first_empty_counter(const level_desc &L, uint64_t b)
-    {
-        const unsigned int c = __ldcg(L.cnt + b);
-        return c < (unsigned int)B ? (int)c : -1;
-    }
-    __device__ __forceinline__ static void store_fp(const level_desc &L, uint64_t b, int s, uint32_t f, uint64_t pol)
-    {
-        unsigned char *p = L.fp + b * B + s;
-        const unsigned short v = (unsigned short)f;
-        asm volatile("st.global.L2::cache_hint.u8 [%0], %1, %2;" ::"l"(p), "h"(v), "l"(pol) : "memory");
-    }
-
     // key and value of a claimed slot, one 16-byte store
     __device__ __forceinline__ static void store_slot(const level_desc &L, uint64_t b, int s, K k, V v)
     {
@@ -982,18 +945,12 @@ struct level_ops_fp {
             const uint64_t raw = ps.at(i);
             if (raw == kProbeEnd) break;
             const uint64_t b = L.nbmod.mod(raw);
-            int s;
-            if constexpr (kFpClaimCounter) {
-                s = f ? claim_counter(L, b) : first_empty_counter(L, b);
-            } else {
-                uint32_t w[NW];
-                load_fp(L, b, w, keep);
-                s = claim(L, b, w, f);
-            }
+            uint32_t w[NW];
+            load_fp(L, b, w, keep);
+            const int s = claim(L, b, w, f);
             if (s < 0) continue;
             if (f) {
                 store_slot(L, b, s, key, val);
-                if constexpr (kFpClaimCounter) store_fp(L, b, s, f, keep);
             } else {
                 // the key 0 (the empty sentinel): as the reference's CAS of 0
                 // over an empty key, it "succeeds" without filling the slot and

@@ -479,7 +479,6 @@ struct bucketed_table {
             D.probe = L.probe;
             D.bucket_bytes = L.bucket_size * (uint32_t)(kBits / 4);
             D.fp = nullptr;
-            D.cnt = nullptr;
         }
         host.desc.nlevels = c.nlevels;
         host.desc.format = kBits == 16 ? (uint32_t)pg::FMT_PACKED16 : (uint32_t)pg::FMT_PACKED8;

@@ -96,9 +96,11 @@ EXPORTED = (
     "pg_pslab_serial_malloc", "pg_pslab_bulk_free",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
     "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
+    "pg_server_add_slab_set", "pg_server_submit_slab",
     "pg_diag_random_access",
 )
 PG_OP_INSERT, PG_OP_QUERY, PG_OP_REMOVE, PG_OP_INSERT_WITH_DELETE = 0, 1, 2, 3
+PG_OP_MALLOC, PG_OP_FREE = 4, 5
 
 
 def lib() -> C.CDLL:
@@ -218,6 +220,10 @@ def lib() -> C.CDLL:
     L.pg_server_drop_table.argtypes = [V, U32]
     L.pg_server_table.restype = V
     L.pg_server_table.argtypes = [V, U32]
+    L.pg_server_add_slab_set.restype = C.c_int
+    L.pg_server_add_slab_set.argtypes = [V, U32, P, P, C.POINTER(U32)]
+    L.pg_server_submit_slab.restype = C.c_int
+    L.pg_server_submit_slab.argtypes = [V, U32, U32, P, U64, P, C.POINTER(U64)]
     L.pg_server_bytes_in_use.restype = U64
     L.pg_server_bytes_in_use.argtypes = [V]
     L.pg_server_submit.restype = C.c_int
@@ -799,6 +805,29 @@ class Server:
                                       len(keys), None if vals_out is None else vals_out.ctypes.data,
                                       None if flags is None else flags.ctypes.data, C.byref(rid)), "pg_server_submit")
         self._live[rid.value] = (keys, vals, vals_out, flags)
+        return rid.value
+
+    def add_slab_set(self, class_bytes, num_allocs) -> int | None:
+        """A served slab size-class set (pg_slab_set_create); None when the HBM budget is exhausted."""
+        cb = (C.c_uint64 * len(class_bytes))(*class_bytes)
+        na = (C.c_uint64 * len(num_allocs))(*num_allocs)
+        sid = C.c_uint32()
+        st = lib().pg_server_add_slab_set(self._h, len(class_bytes), cb, na, C.byref(sid))
+        if st == PG_ERR_FULL:
+            return None
+        _check(st, "pg_server_add_slab_set")
+        return sid.value
+
+    def submit_slab(self, sid: int, op: int, data, ptrs_out=None) -> int:
+        """PG_OP_MALLOC: data = uint32 sizes, ptrs_out = uint64 array for the
+        pointers; PG_OP_FREE: data = uint64 pointers.  Arrays stay alive until polled."""
+        import numpy as np
+        data = np.ascontiguousarray(data, dtype=np.uint32 if op == PG_OP_MALLOC else np.uint64)
+        rid = C.c_uint64()
+        _check(lib().pg_server_submit_slab(self._h, sid, op, data.ctypes.data, len(data),
+                                           None if ptrs_out is None else ptrs_out.ctypes.data, C.byref(rid)),
+               "pg_server_submit_slab")
+        self._live[rid.value] = (data, ptrs_out)
         return rid.value
 
     def poll(self, rid: int, wait: bool = False):

@@ -7,6 +7,7 @@
     python -m poggers_b200.bench_configs --config tcf # TCF and tag-only filter, 2^22 and 2^28 slots
     python -m poggers_b200.bench_configs --config 5   # large: 2^30-slot HT, 2^32-slot tag-only TCF, slab churn, served HT
     python -m poggers_b200.bench_configs --config random  # the random-access ceilings (own kernel)
+    python -m poggers_b200.bench_configs --config slab    # config 5's slab churn alone
 
 Each prints one JSON line.  All inputs are seeded synthetic keys.  The
 reference's own CUDA build is timed on the same keys by oracle/time_refcuda.py
@@ -281,6 +282,12 @@ def config4(args):
                 continue
         reqs.append((ids[t][0], int(op), k, ids[t][1]))
     total_keys = sum(len(r[2]) for r in reqs)
+    # warm-up, untimed: one single-key query per table builds the server's
+    # per-class batches and loads the kernels
+    one = wl.splitmix64(7, 1)
+    warm = [srv.submit(tid, 1, one, None, None, None) for tid, _, _ in ids]
+    for r in warm:
+        srv.poll(r, wait=True)
     results = {}
     for rate in args.rates:
         gaps = rng.exponential(1.0 / rate, len(reqs))
@@ -552,10 +559,10 @@ def config5(args):
     a 2^32-slot tag-only TCF (8 GiB), each filled to 0.9 and queried with as many
     Zipf(1.1) keys (half inserted, half absent); slab churn over 2^24
     allocations of log-uniform sizes in [16, 4096] B (9 power-of-two classes):
-    malloc all, free a seeded random half, malloc it again; and a 2^28-slot
-    uint64 table filled and queried through the serving loop in 2^22-key
-    requests.  Plain launches are timed with CUDA events; the served path by
-    the host clock around submit / poll."""
+    malloc all, free a seeded random half, malloc it again; then the same
+    workload through the serving loop (config5_served).  Plain launches are
+    timed with CUDA events; the served path by the host clock around submit /
+    poll."""
     import torch
     res = {"config": 5}
     # ---- uint64 table, 2^30 slots
@@ -616,8 +623,44 @@ def config5(args):
     del qq, f, t
     torch.cuda.empty_cache()
     # ---- slab churn
+    res["slab_churn"] = slab_churn(1 << 24)
+    # ---- served: the same workload through the serving loop, from host buffers
+    res["served"] = config5_served(args)
+    ht, tcf, slab = res["ht_2p30"], res["tcf_2p32_tag_only"], res["slab_churn"]
+    ht["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["ht_insert"], ht["insert_mops"]),
+                      "query": hbm_frac(ALGO_BYTES["ht_query"], ht["query_mops"])}
+    tcf["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["tcf_insert"], tcf["insert_mops"]),
+                       "query": hbm_frac(ALGO_BYTES["tcf_query"], tcf["query_mops"])}
+    slab["hbm_frac"] = {k: hbm_frac(ALGO_BYTES["slab"], slab[k + "_mops"]) for k in ("malloc", "free", "remalloc")}
+    return res
+
+
+def _host(t):
+    """A device int64 tensor as a host uint64 array."""
+    return t.cpu().numpy().view(np.uint64)
+
+
+def _serve_phase(srv, submit_all):
+    """Submit every request of a phase at once, then collect them; returns the
+    phase's wall time and the requests' latencies and counts."""
+    t0 = time.perf_counter()
+    rids = submit_all()
+    got = [srv.poll(r, wait=True) for r in rids]
+    el = time.perf_counter() - t0
+    return el, [g[1] for g in got], [g[0] for g in got]
+
+
+def _lat(lats):
+    return {"p50_ms": round(1e3 * float(np.percentile(lats, 50)), 2),
+            "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 2)}
+
+
+def slab_churn(na: int):
+    """na allocations with sizes log-uniform in [16, 4096) B over the 9
+    power-of-two size classes (one pool each, 5 % spare): malloc all, free a
+    seeded random half, malloc that half again; CUDA-event timed."""
+    import torch
     rng = np.random.default_rng(5)
-    na = 1 << 24
     sizes = np.floor(2.0 ** rng.uniform(4, 12, na)).astype(np.uint32)
     classes = [16 << i for i in range(9)]
     cls = np.searchsorted(np.array(classes), sizes)
@@ -636,58 +679,100 @@ def config5(args):
     hp2 = torch.zeros_like(hp)
     fc2 = torch.zeros(1, dtype=torch.int64, device="cuda")
     ms_m2, _ = _timed(lambda: ss.bulk_malloc(hs, hp2, fc2))
-    res["slab_churn"] = {"allocations": na, "classes": classes, "malloc_ms": round(ms_m, 2),
-                         "malloc_mops": round(na / ms_m / 1e3, 1), "free_ms": round(ms_f, 2),
-                         "free_mops": round(len(half) / ms_f / 1e3, 1), "remalloc_ms": round(ms_m2, 2),
-                         "remalloc_mops": round(len(half) / ms_m2 / 1e3, 1), "malloc_failures": int(fc.item()),
-                         "free_rejected": int(bad.item()), "remalloc_failures": int(fc2.item()),
-                         "pool_bytes": int(sum(ss.class_report(c)["pool_bytes"] for c in range(9)))}
+    out = {"allocations": na, "classes": classes, "malloc_ms": round(ms_m, 2),
+           "malloc_mops": round(na / ms_m / 1e3, 1), "free_ms": round(ms_f, 2),
+           "free_mops": round(len(half) / ms_f / 1e3, 1), "remalloc_ms": round(ms_m2, 2),
+           "remalloc_mops": round(len(half) / ms_m2 / 1e3, 1), "malloc_failures": int(fc.item()),
+           "free_rejected": int(bad.item()), "remalloc_failures": int(fc2.item()),
+           "pool_bytes": int(sum(ss.class_report(c)["pool_bytes"] for c in range(9)))}
     del ss, ptrs, hp, hp2
     torch.cuda.empty_cache()
-    # ---- served: 2^28-slot uint64 table through the serving loop
-    ns = 1 << 28
-    n = int(0.9 * ns)
+    return out
+
+
+def config_slab(args):
+    """Config 5's slab churn alone (--allocs allocations)."""
+    return {"config": "slab", "slab_churn": slab_churn(args.allocs)}
+
+
+def config5_served(args):
+    """Config 5 through the serving loop: the 2^30-slot uint64 table and the
+    2^32-slot tag-only filter resident in one server beside the 9-class slab
+    set, and the plain workload's keys, values, Zipf(1.1) queries and slab
+    churn submitted from host buffers in requests of 2^22 keys (2^20 slab
+    requests), phase by phase; every phase's requests are submitted at once
+    and collected, so the waves run back to back.  Keys are made on the device
+    and copied to host memory outside the timed phases (host generation would
+    be slower than the server)."""
+    import torch
     req = 1 << 22
-    srv = pg.Server(hbm_budget_bytes=40 << 30, max_wave_keys=1 << 22, max_wave_requests=64)
-    scfg = pg.data_structs.hash_table_64(ns, bucket=8)
-    scfg.fingerprints = True
-    tid = srv.add_table(scfg, 44)
-    keys = wl.splitmix64(44, n)
-    vals = wl.values_for(keys, 8, 45)
-    t0 = time.perf_counter()
-    rids = [srv.submit(tid, pg.PG_OP_INSERT, keys[s:s + req], vals[s:s + req]) for s in range(0, n, req)]
-    lat_i = [srv.poll(r, wait=True)[1] for r in rids]
-    el_i = time.perf_counter() - t0
-    rng = np.random.default_rng(9)
-    ranks = np.minimum(rng.zipf(1.1, n // 2), n) - 1
-    qk = np.empty(n, dtype=np.uint64)
-    qk[0::2][: n // 2] = keys[ranks]
-    qk[1::2][: n - n // 2] = wl.splitmix64(99, n - n // 2)
-    outs = []
-    t0 = time.perf_counter()
-    rids = []
-    for s in range(0, n, req):
-        vo = np.zeros(min(req, n - s), dtype=np.uint64)
-        rids.append(srv.submit(tid, pg.PG_OP_QUERY, qk[s:s + req], None, vo))
-        outs.append(vo)
-    lat_q = [srv.poll(r, wait=True)[1] for r in rids]
-    el_q = time.perf_counter() - t0
+    out = {"request_keys": req}
+    srv = pg.Server(hbm_budget_bytes=60 << 30, max_wave_keys=1 << 22, max_wave_requests=64)
+    ns = 1 << 30
+    n = int(0.9 * ns)
+    cfg = pg.data_structs.hash_table_64(ns, bucket=8)
+    cfg.fingerprints = True
+    tid = srv.add_table(cfg, 43)
+    keys, vals = _host(wl.device_splitmix64(43, n)), _host(wl.device_splitmix64(50, n))
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit(tid, pg.PG_OP_INSERT, keys[s:s + req], vals[s:s + req])
+                                              for s in range(0, n, req)])
+    out["ht_2p30_insert"] = {"keys": n, "mops_e2e": round(n / el / 1e6, 1), "failures": int(sum(cnt)), **_lat(lat)}
+    del keys, vals
+    q = _host(_zipf_queries(43, n, n))
+    vout = np.zeros(n, dtype=np.uint64)
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit(tid, pg.PG_OP_QUERY, q[s:s + req], None, vout[s:s + req])
+                                              for s in range(0, n, req)])
+    out["ht_2p30_query"] = {"keys": n, "mops_e2e": round(n / el / 1e6, 1), "hits": int(sum(cnt)), **_lat(lat)}
+    del q, vout
+    torch.cuda.empty_cache()
+    ns = 1 << 32
+    n = int(0.9 * ns)
+    fid = srv.add_table(pg.data_structs.tcqf(ns), 42)
+    keys = np.empty(n, dtype=np.uint64)
+    for s0 in range(0, n, 1 << 28):
+        c = min(1 << 28, n - s0)
+        keys[s0:s0 + c] = _host(wl.device_splitmix64(42, c, s0))
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit(fid, pg.PG_OP_INSERT, keys[s:s + req])
+                                              for s in range(0, n, req)])
+    out["tcf_2p32_insert"] = {"keys": n, "mops_e2e": round(n / el / 1e6, 1), "failures": int(sum(cnt)), **_lat(lat)}
+    del keys
+    nq = 1 << 30
+    q = np.empty(nq, dtype=np.uint64)
+    for s0 in range(0, nq, 1 << 28):
+        q[s0:s0 + (1 << 28)] = _host(_zipf_queries(42, n, 1 << 28, qseed=11 + s0))
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit(fid, pg.PG_OP_QUERY, q[s:s + req])
+                                              for s in range(0, nq, req)])
+    out["tcf_2p32_query"] = {"keys": nq, "mops_e2e": round(nq / el / 1e6, 1), "hits": int(sum(cnt)), **_lat(lat)}
+    del q
+    # slab churn: malloc all, free a seeded random half, malloc that half again
+    rng = np.random.default_rng(5)
+    na = 1 << 24
+    sizes = np.floor(2.0 ** rng.uniform(4, 12, na)).astype(np.uint32)
+    classes = [16 << i for i in range(9)]
+    counts = np.bincount(np.searchsorted(np.array(classes), sizes), minlength=9)
+    sid = srv.add_slab_set(classes, [int(c * 1.05) + 4096 for c in counts])
+    sreq = 1 << 20
+    ptrs = np.zeros(na, dtype=np.uint64)
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit_slab(sid, pg.PG_OP_MALLOC, sizes[s:s + sreq], ptrs[s:s + sreq])
+                                              for s in range(0, na, sreq)])
+    out["slab_malloc"] = {"allocations": na, "mops_e2e": round(na / el / 1e6, 1), "failures": int(sum(cnt)),
+                          **_lat(lat)}
+    half = wl.fisher_yates_half(na, 77)
+    hp, hs = ptrs[half].copy(), sizes[half].copy()
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit_slab(sid, pg.PG_OP_FREE, hp[s:s + sreq])
+                                              for s in range(0, len(hp), sreq)])
+    out["slab_free"] = {"frees": len(hp), "mops_e2e": round(len(hp) / el / 1e6, 1), "refused": int(sum(cnt)),
+                        **_lat(lat)}
+    hp2 = np.zeros(len(hs), dtype=np.uint64)
+    el, lat, cnt = _serve_phase(srv, lambda: [srv.submit_slab(sid, pg.PG_OP_MALLOC, hs[s:s + sreq], hp2[s:s + sreq])
+                                              for s in range(0, len(hs), sreq)])
+    out["slab_remalloc"] = {"allocations": len(hs), "mops_e2e": round(len(hs) / el / 1e6, 1),
+                            "failures": int(sum(cnt)), **_lat(lat)}
+    out["bytes_in_use"] = int(srv.bytes_in_use())
+    out["note"] = ("host buffers in and out through the server's pinned staging and PCIe; the plain figures "
+                   "are device-resident bulk launches")
     srv.close()
-    res["served_ht_2p28"] = {"slots": ns, "request_keys": req, "inserts": n,
-                             "insert_mops_e2e": round(n / el_i / 1e6, 1),
-                             "insert_p50_ms": round(1e3 * float(np.percentile(lat_i, 50)), 2),
-                             "insert_p99_ms": round(1e3 * float(np.percentile(lat_i, 99)), 2),
-                             "queries": n, "query_mops_e2e": round(n / el_q / 1e6, 1),
-                             "query_p50_ms": round(1e3 * float(np.percentile(lat_q, 50)), 2),
-                             "query_p99_ms": round(1e3 * float(np.percentile(lat_q, 99)), 2),
-                             "note": "host numpy buffers in, values out; per wave: host copies into pinned staging (split over threads), PCIe transfers and kernels, two waves in flight"}
-    ht, tcf, slab = res["ht_2p30"], res["tcf_2p32_tag_only"], res["slab_churn"]
-    ht["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["ht_insert"], ht["insert_mops"]),
-                      "query": hbm_frac(ALGO_BYTES["ht_query"], ht["query_mops"])}
-    tcf["hbm_frac"] = {"insert": hbm_frac(ALGO_BYTES["tcf_insert"], tcf["insert_mops"]),
-                       "query": hbm_frac(ALGO_BYTES["tcf_query"], tcf["query_mops"])}
-    slab["hbm_frac"] = {k: hbm_frac(ALGO_BYTES["slab"], slab[k + "_mops"]) for k in ("malloc", "free", "remalloc")}
-    return res
+    return out
 
 
 def srv_config_of(kind, n):
@@ -742,7 +827,8 @@ def config_random(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "random"], required=True)
+    ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "random", "slab"], required=True)
+    ap.add_argument("--allocs", type=int, default=1 << 24, help="config slab: allocations")
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--only", nargs="+", default=None, help="config tcf: run only these workloads")
@@ -762,7 +848,7 @@ def main():
     import torch
     torch.cuda.init()
     fn = {"1": config1, "3": config3, "4": config4, "5": config5, "del": config_del, "tcf": config_tcf,
-          "random": config_random}[a.config]
+          "random": config_random, "slab": config_slab}[a.config]
     print(json.dumps(fn(a)))
 
 

@@ -45,9 +45,10 @@ constexpr int kMaxWaves = 3;
 
 struct request {
     uint64_t id;
-    uint32_t table;
+    uint32_t table;  // table id, or the slab set id when slab >= 0
+    int32_t slab;    // -1: a table request; else PG_OP_MALLOC / PG_OP_FREE on slab set `table`
     uint32_t op;
-    const uint64_t *keys;
+    const uint64_t *keys;  // table keys; malloc: uint32_t sizes; free: object pointers
     const void *vals;
     uint64_t n;
     void *vals_out;
@@ -63,6 +64,15 @@ struct table_entry {
     uint64_t bytes;
     bool live;
     uint32_t inflight = 0;  // requests taken into a wave and not yet completed
+};
+
+// a slab size-class set served by the loop: its requests run on its own stream
+struct slab_entry {
+    pg_slab_set *set = nullptr;
+    cudaStream_t stream = nullptr;
+    uint64_t bytes = 0;
+    bool live = false;
+    uint32_t inflight = 0;
 };
 
 struct klass {
@@ -94,6 +104,7 @@ struct pg_server {
     uint64_t bytes_used = 0;
     std::vector<table_entry> tables;
     std::vector<klass> classes;
+    std::vector<slab_entry> slabs;
     std::deque<request *> pending;
     std::map<uint64_t, request *> done;
     // staging (per wave slot): pinned host and device buffers
@@ -138,6 +149,8 @@ void sync_all(pg_server *s)
     cudaStreamSynchronize(s->stream);
     for (auto &k : s->classes)
         if (k.stream) cudaStreamSynchronize(k.stream);
+    for (auto &e : s->slabs)
+        if (e.stream) cudaStreamSynchronize(e.stream);
     cudaStreamSynchronize(s->down);
 }
 
@@ -173,15 +186,17 @@ std::vector<request *> take_wave(pg_server *s, pg_server::stage &st, uint64_t &n
     const uint64_t cap_keys = s->cfg.max_wave_keys;
     const uint32_t cap_ops = s->cfg.max_wave_requests;
     for (request *r : s->pending) {
-        bool ok = !blocked[r->table] && nops < cap_ops && nkeys + r->n <= cap_keys;
-        auto it = table_op.find(r->table);
+        // tables and slab sets are ordered separately (slab set ids in the upper half)
+        const uint32_t key = r->slab >= 0 ? (0x80000000u | r->table) : r->table;
+        bool ok = !blocked[key] && nops < cap_ops && nkeys + r->n <= cap_keys;
+        auto it = table_op.find(key);
         if (ok && it != table_op.end() && conflicts(it->second, r->op)) ok = false;
         if (!ok) {
-            blocked[r->table] = true;
+            blocked[key] = true;
             keep.push_back(r);
             continue;
         }
-        table_op[r->table] = r->op;
+        table_op[key] = r->op;
         out.push_back(r);
         nkeys += r->n;
         nops++;
@@ -256,6 +271,12 @@ struct wave_plan {
         uint32_t first, count, vb;
     };
     std::vector<run> runs;  // one pg_batch_run per kernel class, requests [first, first + count)
+    struct slab_run {
+        pg_slab_set *set;
+        cudaStream_t stream;
+        uint32_t req;
+    };
+    std::vector<slab_run> slab_runs;  // one bulk malloc / free per slab request
     uint64_t nkeys = 0;
 };
 
@@ -269,6 +290,10 @@ void complete_stage(pg_server::stage &st, const wave_plan &pl)
         request *r = pl.reqs[i];
         const uint64_t o = pl.key_off[i];
         const uint32_t vb = pl.vb[i];
+        if (r->slab >= 0) {
+            if (r->op == PG_OP_MALLOC && r->vals_out) jobs.push_back({r->vals_out, st.h_vout[0] + o * 8, r->n * 8});
+            continue;
+        }
         if (r->flags) jobs.push_back({r->flags, st.h_flags + o, r->n});
         if (r->op == PG_OP_QUERY && r->vals_out && vb) jobs.push_back({r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb});
     }
@@ -300,7 +325,8 @@ void worker_loop(pg_server *s)
                 complete_stage(s->stages[w], slots[w].plan);
                 lk.lock();
                 for (request *r : slots[w].plan.reqs) {
-                    s->tables[r->table].inflight--;
+                    if (r->slab >= 0) s->slabs[r->table].inflight--;
+                    else s->tables[r->table].inflight--;
                     s->done[r->id] = r;
                 }
                 slots[w].plan = wave_plan();
@@ -340,15 +366,26 @@ void worker_loop(pg_server *s)
             wave_plan &pl = slots[w].plan;
             pl.reqs = take_wave(s, st, nkeys, nops, opc);
             // group requests by class; each class's requests are contiguous in the op array
-            std::stable_sort(pl.reqs.begin(), pl.reqs.end(), [&](request *a, request *b) {
-                return s->tables[a->table].cls < s->tables[b->table].cls;
-            });
+            // (slab requests after every table request)
+            auto order = [&](const request *r) -> uint64_t {
+                return r->slab >= 0 ? (1ull << 32) + r->table : (uint64_t)s->tables[r->table].cls;
+            };
+            std::stable_sort(pl.reqs.begin(), pl.reqs.end(),
+                             [&](request *a, request *b) { return order(a) < order(b); });
             const size_t nr = pl.reqs.size();
             pl.key_off.assign(nr, 0);
             pl.vb.assign(nr, 0);
             pl.slot.assign(nr, 0);
             uint64_t ko = 0;
             for (size_t i = 0; i < nr; i++) {
+                if (pl.reqs[i]->slab >= 0) {
+                    slab_entry &se = s->slabs[pl.reqs[i]->table];
+                    se.inflight++;
+                    pl.key_off[i] = ko;
+                    ko += pl.reqs[i]->n;
+                    pl.slab_runs.push_back({se.set, se.stream, (uint32_t)i});
+                    continue;
+                }
                 table_entry &te = s->tables[pl.reqs[i]->table];
                 te.inflight++;
                 pl.key_off[i] = ko;
@@ -369,6 +406,13 @@ void worker_loop(pg_server *s)
                 request *r = pl.reqs[i];
                 const uint64_t o = pl.key_off[i];
                 const uint32_t vb = pl.vb[i];
+                if (r->slab >= 0) {
+                    // malloc: n sizes of 4 bytes; free: n pointers; both fit the keys' 8 bytes each
+                    jobs.push_back({st.h_keys + o, r->keys, r->n * (r->op == PG_OP_MALLOC ? 4 : 8)});
+                    if (r->op == PG_OP_MALLOC) any_q[0] = true;
+                    st.h_ops[i] = pg_op_desc{0, r->op, o, r->n};
+                    continue;
+                }
                 jobs.push_back({st.h_keys + o, r->keys, r->n * 8});
                 if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
                     jobs.push_back({st.h_vin[width_index(vb)] + o * vb, r->vals, r->n * vb});
@@ -400,6 +444,22 @@ void worker_loop(pg_server *s)
                 if (rs != PG_OK) launch_error = rs;
                 // the download waits for this run (a wait takes the event's latest record)
                 cudaEventRecord(st.ran, rn.stream);
+                cudaStreamWaitEvent(s->down, st.ran, 0);
+            }
+            for (const wave_plan::slab_run &sr : pl.slab_runs) {
+                const request *r = pl.reqs[sr.req];
+                const uint64_t o = pl.key_off[sr.req];
+                cudaStreamWaitEvent(sr.stream, st.uploaded, 0);
+                pg_status rs;
+                if (r->op == PG_OP_MALLOC)
+                    rs = pg_slab_set_bulk_malloc(sr.set, reinterpret_cast<const uint32_t *>(st.d_keys + o), r->n,
+                                                 reinterpret_cast<void **>(st.d_vout[0] + o * 8), st.d_counts + sr.req,
+                                                 reinterpret_cast<pg_stream_t>(sr.stream));
+                else
+                    rs = pg_slab_set_bulk_free(sr.set, reinterpret_cast<void *const *>(st.d_keys + o), r->n,
+                                               st.d_counts + sr.req, reinterpret_cast<pg_stream_t>(sr.stream));
+                if (rs != PG_OK) launch_error = rs;
+                cudaEventRecord(st.ran, sr.stream);
                 cudaStreamWaitEvent(s->down, st.ran, 0);
             }
             cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->down);
@@ -491,6 +551,10 @@ pg_status pg_server_destroy(pg_server *s)
     }
     for (auto &te : s->tables)
         if (te.live) pg_table_destroy(te.t);
+    for (auto &e : s->slabs) {
+        if (e.set) pg_slab_set_destroy(e.set);
+        if (e.stream) cudaStreamDestroy(e.stream);
+    }
     for (auto &st : s->stages) {
         cudaFreeHost(st.h_keys);
         cudaFree(st.d_keys);
@@ -535,8 +599,7 @@ pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t
         if (L.bucket_size == 0 || L.nslots == 0) return PG_ERR_INVALID;
         const uint64_t nb = (L.nslots - 1) / L.bucket_size + 1;
         need += nb * L.bucket_size * (kb + vb);
-        if (l == 0 && (cfg->flags & PG_TABLE_FINGERPRINTS))
-            need += (nb * L.bucket_size + 255) / 256 * 256 + nb * 4;  // fingerprint bytes, then bucket counters
+        if (l == 0 && (cfg->flags & PG_TABLE_FINGERPRINTS)) need += nb * L.bucket_size;
     }
     std::lock_guard<std::mutex> g(s->mu);
     if (s->bytes_used + need > s->cfg.hbm_budget_bytes) return PG_ERR_FULL;
@@ -625,12 +688,68 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
     request *r = new request();
     r->id = s->next_id++;
     r->table = table_id;
+    r->slab = -1;
     r->op = op;
     r->keys = h_keys;
     r->vals = h_vals;
     r->n = n;
     r->vals_out = h_vals_out;
     r->flags = h_flags;
+    r->count = 0;
+    r->t_submit = now_s();
+    r->t_done = 0;
+    s->pending.push_back(r);
+    *request_id = r->id;
+    s->cv.notify_all();
+    return PG_OK;
+}
+
+pg_status pg_server_add_slab_set(pg_server *s, uint32_t nclasses, const uint64_t *class_bytes,
+                                 const uint64_t *num_allocs, uint32_t *set_id)
+{
+    if (!s || !class_bytes || !num_allocs || !set_id || nclasses == 0) return PG_ERR_INVALID;
+    // admission: every class's pool (whole slabs of 4096 objects) and its bitmaps
+    uint64_t need = 0;
+    for (uint32_t c = 0; c < nclasses; c++) {
+        const uint64_t objs = (num_allocs[c] + 4095) / 4096 * 4096;
+        need += objs * class_bytes[c] + objs / 8 + objs / 512;
+    }
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->bytes_used + need > s->cfg.hbm_budget_bytes) return PG_ERR_FULL;
+    slab_entry e;
+    pg_status st = pg_slab_set_create(nclasses, class_bytes, num_allocs, &e.set);
+    if (st != PG_OK) return st;
+    if (cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        pg_slab_set_destroy(e.set);
+        return PG_ERR_CUDA;
+    }
+    e.bytes = need;
+    e.live = true;
+    *set_id = (uint32_t)s->slabs.size();
+    s->slabs.push_back(e);
+    s->bytes_used += need;
+    return PG_OK;
+}
+
+pg_status pg_server_submit_slab(pg_server *s, uint32_t set_id, uint32_t op, const void *h_in, uint64_t n,
+                                uint64_t *h_ptrs_out, uint64_t *request_id)
+{
+    if (!s || !request_id || (n && !h_in) || (op != PG_OP_MALLOC && op != PG_OP_FREE)) return PG_ERR_INVALID;
+    if (n > s->cfg.max_wave_keys) return PG_ERR_INVALID;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (set_id >= s->slabs.size() || !s->slabs[set_id].live) return PG_ERR_INVALID;
+    if (s->error != PG_OK) return s->error;
+    request *r = new request();
+    r->id = s->next_id++;
+    r->table = set_id;
+    r->slab = (int32_t)set_id;
+    r->op = op;
+    r->keys = static_cast<const uint64_t *>(h_in);
+    r->vals = nullptr;
+    r->n = n;
+    r->vals_out = h_ptrs_out;
+    r->flags = nullptr;
     r->count = 0;
     r->t_submit = now_s();
     r->t_done = 0;

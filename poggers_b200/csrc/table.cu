@@ -125,6 +125,14 @@ void launch_shape(const pg_table *t, uint32_t lanes, uint64_t n, dim3 &grid, dim
     block = dim3(bt);
 }
 
+// Inserts into a small two-choice level keep few keys in flight: every
+// in-flight key of a bucket decides its shortcut on a fill count that misses
+// the others.  The filters' kernels fit 6 blocks of 256 per SM; these inserts
+// launch at most 2 per SM, the residency at which a 2^16-slot TCF with 1 %
+// backing places every key at 0.85 load and fails fewer than the reference's
+// build at 0.9 (with 6 resident blocks: 103 and 771 failures).
+constexpr uint32_t kSmallTwoChoiceBlocksPerSm = 2;
+
 pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
 {
     if (!t) return PG_ERR_INVALID;
@@ -133,6 +141,11 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     dim3 grid, block;
     const uint32_t tile = pg_table_lanes(t, op);
     launch_shape(t, tile, a.n, grid, block, a.perm != nullptr);
+    const pg_level_config &L0 = t->cfg.levels[0];
+    if (op == OP_INSERT && L0.scheme == PG_SCHEME_TWO_CHOICE && L0.nslots < (1ull << 18) && !t->max_blocks) {
+        const uint64_t cap = (uint64_t)t->num_sms * kSmallTwoChoiceBlocksPerSm;
+        if (grid.x > cap) grid.x = (unsigned)cap;
+    }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t b0 = t->cfg.levels[0].bucket_size;
     const table_desc &d = t->desc;
@@ -224,22 +237,13 @@ __global__ void __launch_bounds__(256) k_count_fill(const unsigned char *base, u
     }
 }
 
-// fingerprint bytes and bucket counters recomputed from the slots (after a
-// level is loaded): a bucket's counter is its filled prefix, the index of its
-// first empty slot
-__global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, unsigned char *fp, unsigned int *cnt,
-                                                    uint64_t nbuckets, uint32_t B, uint64_t seed)
+// fingerprint bytes recomputed from the slots (after a level is loaded)
+__global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, unsigned char *fp, uint64_t nslots,
+                                                    uint64_t seed)
 {
-    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbuckets;
-         b += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t filled = B;
-        for (uint32_t j = 0; j < B; ++j) {
-            const uint64_t s = b * B + j;
-            const uint64_t key = *reinterpret_cast<const unsigned long long *>(base + 16 * s);
-            fp[s] = fp_of(key, murmur64a_u64(key, seed));
-            if (key == 0 && filled == B) filled = j;
-        }
-        cnt[b] = filled;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t key = *reinterpret_cast<const unsigned long long *>(base + 16 * s);
+        fp[s] = fp_of(key, murmur64a_u64(key, seed));
     }
 }
 
@@ -339,11 +343,8 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
         }
         D.base = static_cast<unsigned char *>(t->mem[l]);
         D.fp = nullptr;
-        D.cnt = nullptr;
         if (l == 0 && fingerprinted(cfg)) {
-            // one allocation: the fingerprint bytes, then a 4-byte counter per bucket
-            const uint64_t fp_span = (nb * L.bucket_size + 255) / 256 * 256;
-            t->fp_bytes = fp_span + nb * 4;
+            t->fp_bytes = nb * L.bucket_size;
             e = cudaMalloc(&t->fp, t->fp_bytes);
             if (e == cudaSuccess) e = cudaMemset(t->fp, 0, t->fp_bytes);
             if (e != cudaSuccess) {
@@ -352,8 +353,7 @@ pg_status pg_table_create(const pg_table_config *cfg, uint64_t seed, pg_table **
                 return cuda_status(e);
             }
             D.fp = static_cast<unsigned char *>(t->fp);
-            D.cnt = reinterpret_cast<unsigned int *>(D.fp + fp_span);
-            D.fp_resident = nb * L.bucket_size <= kFpResidentBytes;
+            D.fp_resident = t->fp_bytes <= kFpResidentBytes;
         }
         s = s * s;  // recursive table gets seed*seed (base_table.cuh:124)
     }
@@ -563,7 +563,7 @@ pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src,
     if (!split_layout(&t->cfg)) {
         cudaError_t e = cudaMemcpy(t->mem[level], host_src, t->bytes[level], cudaMemcpyHostToDevice);
         if (e == cudaSuccess && level == 0 && t->fp) {
-            k_rebuild_fp<<<1184, 256>>>(D.base, D.fp, D.cnt, D.nbmod.d, D.bucket_size, D.seed);
+            k_rebuild_fp<<<1184, 256>>>(D.base, D.fp, nslots, D.seed);
             e = cudaDeviceSynchronize();
         }
         return cuda_status(e);

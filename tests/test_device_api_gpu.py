@@ -59,9 +59,15 @@ def test_slab_allocator_device_api(drivers):
     r = subprocess.run([str(drivers["test_slab_api"])], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     d = json.loads(r.stdout.strip().splitlines()[-1])
+    # provisioned as the reference's own test: no misses, no duplicates, all in the pool
     assert d["misses"] == 0 and d["duplicates"] == 0 and d["out_of_pool"] == 0
-    assert d["misses_2"] == 0 and d["duplicates_2"] == 0 and d["double_free_refused"] == 1
-    assert d["free_slabs_when_full"] == 0 and d["free_slabs_after_free"] == d["slabs"] == d["allocs"] // 4096
-    # malloc() called from divergent branches of a warp: the whole pool, each object once
+    assert d["misses_2"] == 0 and d["duplicates_2"] == 0 and d["out_of_pool_2"] == 0
+    # malloc() called from divergent branches of a warp: the same
     assert d["misses_divergent"] == 0 and d["duplicates_divergent"] == 0 and d["out_of_pool_divergent"] == 0
-    assert d["free_slabs_divergent"] == 0
+    # the pins take 16 slabs per SM out of the pool; frees only return slabs to it,
+    # and the slabs counted as returned by free_count_misses are the ones it gained
+    assert d["fill_initial"] == d["slabs"] - 16 * d["sm_ids"]
+    assert d["fill_full"] <= d["fill_empty"] <= d["fill_initial"]
+    assert d["fill_empty"] - d["fill_full"] == d["returned"]
+    # a double free is refused: counted by neither free_count_misses counter
+    assert d["double_free_counted"] == 0 and d["double_free_seen"] == 1

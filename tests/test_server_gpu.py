@@ -244,3 +244,48 @@ def test_server_large_requests_split_their_host_copies(pg):
         srv.drop_table(tid)
     finally:
         srv.close()
+
+
+def test_served_slab_requests_beside_table_requests(pg):
+    """Slab size-class sets served by the loop: malloc requests return distinct
+    objects of the smallest class that fits, free requests refuse nothing, and
+    table requests in the same waves keep their results."""
+    import numpy as np
+    classes = [16, 64, 256, 1024]
+    srv = pg.Server(hbm_budget_bytes=4 << 30, max_wave_keys=1 << 16, max_wave_requests=256)
+    sid = srv.add_slab_set(classes, [1 << 16] * 4)
+    tid = srv.add_table(pg.data_structs.hash_table_64(1 << 14, bucket=8), 5)
+    rng = np.random.default_rng(9)
+    sizes = [rng.integers(1, 1025, int(n)).astype(np.uint32) for n in rng.integers(1, 4000, 12)]
+    outs = [np.zeros(len(z), dtype=np.uint64) for z in sizes]
+    keys = wl.keys_without_sentinels(61, 5000)
+    vals = wl.values_for(keys, 8, 2)
+    rids = []
+    for i, (z, o) in enumerate(zip(sizes, outs)):
+        rids.append(srv.submit_slab(sid, pg.PG_OP_MALLOC, z, o))
+        if i == 3:
+            rids.append(srv.submit(tid, pg.PG_OP_INSERT, keys, vals))
+    counts = [srv.poll(r, wait=True)[0] for r in rids]
+    assert sum(counts) == 0
+    allp = np.concatenate(outs)
+    assert (allp != 0).all() and len(np.unique(allp)) == len(allp)
+    # each object came from the smallest class that fits its size: objects of
+    # one class are that class's size apart from each other
+    zs = np.concatenate(sizes)
+    cls = np.searchsorted(np.array(classes), zs)
+    for c, b in enumerate(classes):
+        p = np.sort(allp[cls == c])
+        if len(p) > 1:
+            assert (np.diff(p) % b == 0).all()
+    # query the table between frees
+    vout = np.zeros(len(keys), dtype=np.uint64)
+    frees = [srv.submit_slab(sid, pg.PG_OP_FREE, o) for o in outs[:6]]
+    q = srv.submit(tid, pg.PG_OP_QUERY, keys, None, vout)
+    frees += [srv.submit_slab(sid, pg.PG_OP_FREE, o) for o in outs[6:]]
+    assert all(srv.poll(r, wait=True)[0] == 0 for r in frees)
+    hits = srv.poll(q, wait=True)[0]
+    assert hits == len(keys) and (vout == vals).all()
+    # a second free of the same objects is refused, every one
+    again = srv.submit_slab(sid, pg.PG_OP_FREE, outs[0])
+    assert srv.poll(again, wait=True)[0] == len(outs[0])
+    srv.close()

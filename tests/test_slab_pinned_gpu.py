@@ -61,8 +61,10 @@ def test_serial_sequence_matches_the_reference_restatement(pg, oracle, group, ex
     p = ptrs.cpu().numpy().view(np.uint64)
     live = p[p != 0]
     assert len(live) == len(got) and len(np.unique(live)) == len(live)
+    # the pool's three slabs are spent -- unless there is no backup place to
+    # refill (extra_blocks 0), in which case the pool is never used
     info_pool = pool.report()
-    assert info_pool["report_fill"] == ref.report_fill() == 0
+    assert info_pool["report_fill"] == ref.report_fill() == (3 if extra == 0 else 0)
     # free everything in order: the same counts of frees, returned slabs and
     # slabs emptied while pinned as the reference's free_count_misses
     counts = torch.zeros(4, dtype=torch.int64, device="cuda")
