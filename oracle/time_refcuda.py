@@ -101,7 +101,7 @@ def time_config3(args):
     from oracle import pyrefcuda as rc
     from poggers_b200 import bench_configs as bc
 
-    d = bc.config3_inputs(args.tables)
+    d = bc.config3_inputs(args.tables or 1024)
     offs, counts = d["offs"], d["counts"]
     dk, dv, dq = bc._dev(d["ins"]), bc._dev(d["vals"]), bc._dev(d["q"])
     N = len(d["ins"])
@@ -201,7 +201,7 @@ def time_config5(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=["del", "tcf", "3", "5"], required=True)
-    ap.add_argument("--tables", type=int, default=1024, help="config 3: number of tables")
+    ap.add_argument("--tables", type=int, default=None, help="config 3: number of tables (1024)")
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     a = ap.parse_args()

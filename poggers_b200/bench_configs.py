@@ -129,7 +129,7 @@ def config3(args):
     the timed region, for both paths."""
     import torch
     from poggers_b200 import autotune as at
-    ntab = args.tables
+    ntab = args.tables or 1024
     d = config3_inputs(ntab)
     sizes, counts, offs = d["sizes"], d["counts"], d["offs"]
     dk, dv, dq = _dev(d["ins"]), _dev(d["vals"]), _dev(d["q"])
@@ -238,7 +238,7 @@ def config4(args):
     p50/p99 latency at each offered rate, and the plain per-request path."""
     import torch
     rng = np.random.default_rng(4)
-    ntab = args.tables
+    ntab = args.tables or 256
     budget = int(args.budget_gb * (1 << 30))
     per = budget // ntab
     kinds = ["tcf" if i % 2 else "ht" for i in range(ntab)]
@@ -797,6 +797,17 @@ def config_random(args):
     import torch
     modes = {"read32": pg.PG_DIAG_READ32, "read64": pg.PG_DIAG_READ64, "read32_cas": pg.PG_DIAG_READ32_CAS,
              "red32": pg.PG_DIAG_RED32}
+    if args.calibrate:
+        # one launch per kind over a 1 GiB and a 32 MiB buffer (for an ncu capture of DRAM and L2 traffic)
+        done = {}
+        for lg in (30, 25):
+            buf = torch.zeros(1 << lg, dtype=torch.uint8, device="cuda")
+            for name, mode in modes.items():
+                done[f"{(1 << lg) >> 20}MiB_{name}"] = pg.diag_random_access(buf, mode, 1 << 26, seed=mode + 1,
+                                                                               blocks_per_sm=8)
+                torch.cuda.synchronize()
+            del buf
+        return {"config": "random", "calibrate": done}
     sectors = {"read32": 1, "read64": 2, "read32_cas": 1, "red32": 1}
     out = {"config": "random", "note": "G accesses/s; sector_g_per_s counts the 32-byte sectors read per access"}
     sink = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -829,11 +840,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", choices=["1", "3", "4", "5", "del", "tcf", "random", "slab"], required=True)
     ap.add_argument("--allocs", type=int, default=1 << 24, help="config slab: allocations")
+    ap.add_argument("--calibrate", action="store_true", help="config random: one launch per kind (ncu captures)")
     ap.add_argument("--log2", type=int, default=28, help="config del: log2 of the primary slot count")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--only", nargs="+", default=None, help="config tcf: run only these workloads")
     ap.add_argument("--tcf-log2", type=int, default=0, help="config tcf: log2 slots instead of each workload's own")
-    ap.add_argument("--tables", type=int, default=1024)
+    ap.add_argument("--tables", type=int, default=None, help="tables (config 3: 1024, config 4: 256)")
     ap.add_argument("--lanes-grid", type=int, nargs="+", default=None, help="config 3: the tuner's lanes per key")
     ap.add_argument("--bucket-grid", type=int, nargs="+", default=None, help="config 3: the tuner's bucket sizes")
     ap.add_argument("--bps-grid", type=int, nargs="+", default=None, help="config 3: the tuner's blocks per SM")

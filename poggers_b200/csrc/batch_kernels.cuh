@@ -42,7 +42,7 @@ struct batch_args {
 __global__ void __launch_bounds__(1024) k_batch_plan(batch_args a);
 
 template <int FMT, int B, int G, int S0, bool BK>
-__global__ void __launch_bounds__(256, min_blocks_of<FMT>()) k_batch(batch_args a)
+__global__ void __launch_bounds__(256, min_blocks_of<FMT, G>()) k_batch(batch_args a)
 {
     using F = fmt_t<FMT>;
     using V = typename F::V;

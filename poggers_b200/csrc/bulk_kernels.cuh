@@ -58,16 +58,19 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 #ifndef PG_FILTER_MIN_BLOCKS
 #define PG_FILTER_MIN_BLOCKS 6
 #endif
-template <int FMT>
+// Only the one-lane filter kernels (large tables) are held: the 4-lane ones
+// serve two-choice levels below 2^18 slots, which launch few blocks anyway,
+// and at 40 registers they would spill ~0.7 KB per thread.
+template <int FMT, int G = 1>
 constexpr int min_blocks_of()
 {
     if (FMT == FMT_KV64_FP) return 8;
-    if (FMT == FMT_TAGVAL16 || FMT == FMT_TAGVAL16_SPLIT || FMT == FMT_TAG16) return PG_FILTER_MIN_BLOCKS;
+    if ((FMT == FMT_TAGVAL16 || FMT == FMT_TAGVAL16_SPLIT || FMT == FMT_TAG16) && G == 1) return PG_FILTER_MIN_BLOCKS;
     return PG_MIN_BLOCKS;
 }
 
 template <int FMT, int B, int G, int S0, bool BK, int OP>
-__global__ void __launch_bounds__(256, min_blocks_of<FMT>()) k_bulk(table_desc t, bulk_args a)
+__global__ void __launch_bounds__(256, min_blocks_of<FMT, G>()) k_bulk(table_desc t, bulk_args a)
 {
     using F = fmt_t<FMT>;
     using V = typename F::V;
