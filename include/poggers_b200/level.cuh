@@ -406,7 +406,13 @@ struct level_ops {
         int np = 0, min_fill = B;
         snap k1;
         bool act1 = false, have1 = false;
-        if (kTwoChoicePrefetch && L.max_probes >= 2 && ps.at(0) != kProbeEnd && ps.at(1) != kProbeEnd) {
+        // Groups of several lanes serve two-choice levels below 2^18 slots
+        // (pg_table_lanes): there both choices are read together, so a key's
+        // two fills come from one moment.  With the second read deferred, a
+        // 2^16-slot TCF with 1 % backing failed 209-217 keys at 0.9 load,
+        // against none with both read together (the reference's build: ~100).
+        constexpr bool kPrefetch = kTwoChoicePrefetch || G > 1;
+        if (kPrefetch && L.max_probes >= 2 && ps.at(0) != kProbeEnd && ps.at(1) != kProbeEnd) {
             load(L, g, L.nbmod.mod(ps.at(1)), k1, act1);
             have1 = true;
         }
