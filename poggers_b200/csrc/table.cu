@@ -125,14 +125,6 @@ void launch_shape(const pg_table *t, uint32_t lanes, uint64_t n, dim3 &grid, dim
     block = dim3(bt);
 }
 
-// Inserts into a small two-choice level keep few keys in flight: every
-// in-flight key of a bucket decides its shortcut on a fill count that misses
-// the others.  The filters' kernels fit 6 blocks of 256 per SM; these inserts
-// launch at most 2 per SM, the residency at which a 2^16-slot TCF with 1 %
-// backing places every key at 0.85 load and fails fewer than the reference's
-// build at 0.9 (with 6 resident blocks: 103 and 771 failures).
-constexpr uint32_t kSmallTwoChoiceBlocksPerSm = 2;
-
 pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
 {
     if (!t) return PG_ERR_INVALID;
@@ -141,11 +133,6 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
     dim3 grid, block;
     const uint32_t tile = pg_table_lanes(t, op);
     launch_shape(t, tile, a.n, grid, block, a.perm != nullptr);
-    const pg_level_config &L0 = t->cfg.levels[0];
-    if (op == OP_INSERT && L0.scheme == PG_SCHEME_TWO_CHOICE && L0.nslots < (1ull << 18) && !t->max_blocks) {
-        const uint64_t cap = (uint64_t)t->num_sms * kSmallTwoChoiceBlocksPerSm;
-        if (grid.x > cap) grid.x = (unsigned)cap;
-    }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t b0 = t->cfg.levels[0].bucket_size;
     const table_desc &d = t->desc;
