@@ -195,15 +195,20 @@ pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t
  * holds the keys expected in its region plus a margin; the keys a run cannot
  * hold (a batch far from uniform over the table) are inserted afterwards in
  * batch order.  The sort costs about 20 bytes of device scratch per key,
- * allocated by the first such insert and kept by the table (counted in
- * pg_table_bytes) until pg_table_destroy.
+ * kept by the table (counted in pg_table_bytes) until pg_table_destroy.  The
+ * first such insert (or one larger than any before) grows it with a
+ * stream-ordered allocation on the insert's stream (cudaMallocAsync: no
+ * device-wide synchronization); pg_table_reserve_insert_scratch grows it
+ * ahead of time, so that no insert allocates.
  * Concurrent inserts have no defined order in the reference either: which
  * keys fail when a table overflows may differ, every placed key is
  * placed by the same rule.  The scratch is the table's: two region-ordered
- * inserts into one table must be ordered on one stream, and the first one
- * (or one larger than any before) allocates, so make it before any stream
- * capture or turn region ordering off. */
+ * inserts into one table must be ordered on one stream. */
 pg_status pg_table_set_partitioned_insert(pg_table *t, int enable);
+/* Grow the region sort's scratch for insert batches of up to max_batch_keys
+ * keys (ordered on `stream`); PG_ERR_NOMEM if it cannot be allocated.  No
+ * counterpart in the reference. */
+pg_status pg_table_reserve_insert_scratch(pg_table *t, uint64_t max_batch_keys, pg_stream_t stream);
 
 /* Bulk insert of n keys (and values; d_vals may be NULL = all 0).
  * d_ok[i] (optional) = 1 if key i was placed; d_fail_count (optional) += failures.

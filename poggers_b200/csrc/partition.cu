@@ -227,35 +227,62 @@ using namespace pg;
 // a run; its extra keys are inserted by the second pass, in batch order.
 namespace {
 
-bool region_sort(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t s)
+// The sort's plan for a batch of n keys: regions of 2^shift buckets (about
+// kPartRegionBytes of slots each, at most kPartMaxRegions), run capacity, the
+// entries of the sorted copy and the scratch bytes.  False when the batch
+// takes the ordinary path.
+struct region_plan {
+    uint32_t shift, R;
+    uint64_t cap, nv, cur_off, ovf_off, need;
+};
+
+bool plan_regions(const pg_table *t, uint64_t n, region_plan &pl)
 {
-    const uint64_t n = a.n;
     if (t->bytes[0] < 2 * kPartRegionBytes || n < kPartMinKeys || n >= (1ull << 32)) return false;
-    // regions of 2^shift buckets, about kPartRegionBytes of slots each, at most kPartMaxRegions
     const uint64_t nb = t->desc.lv[0].nbmod.d, bucket_bytes = t->bytes[0] / nb;
     uint32_t shift = 0;
     while ((bucket_bytes << (shift + 1)) <= kPartRegionBytes) shift++;
     while (((nb - 1) >> shift) + 1 > kPartMaxRegions) shift++;
     const uint32_t R = (uint32_t)(((nb - 1) >> shift) + 1);
     const double expect = (double)n * (double)(1ull << shift) / (double)nb;
-    const uint64_t cap = (uint64_t)(expect + 8.0 * sqrt(expect)) + 1024;
-    const uint64_t nv = cap * R;  // entries of the sorted copy, runs included
-    if (nv >= (1ull << 32)) return false;
+    pl.shift = shift;
+    pl.R = R;
+    pl.cap = (uint64_t)(expect + 8.0 * sqrt(expect)) + 1024;
+    pl.nv = pl.cap * R;  // entries of the sorted copy, runs included
+    if (pl.nv >= (1ull << 32)) return false;
     // scratch: keys (8 B), values (8 B) and original index (4 B) per entry;
     // run cursors; one overflow bit per key of the batch
-    const uint64_t cur_off = (nv * 20 + 255) & ~255ull;
-    const uint64_t ovf_off = cur_off + ((R * 8ull + 255) & ~255ull);
-    const uint64_t need = ovf_off + ((n + 31) / 32) * 4;
-    if (t->part_bytes < need) {
-        if (t->part_buf) cudaFree(t->part_buf);
+    pl.cur_off = (pl.nv * 20 + 255) & ~255ull;
+    pl.ovf_off = pl.cur_off + ((R * 8ull + 255) & ~255ull);
+    pl.need = pl.ovf_off + ((n + 31) / 32) * 4;
+    return true;
+}
+
+// Grow the table's sort scratch to `need` bytes, ordered on stream s (a
+// stream-ordered free and allocation: no device-wide synchronization).
+bool grow_scratch(pg_table *t, uint64_t need, cudaStream_t s)
+{
+    if (t->part_bytes >= need) return true;
+    if (t->part_buf) cudaFreeAsync(t->part_buf, s);
+    t->part_buf = nullptr;
+    t->part_bytes = 0;
+    if (cudaMallocAsync(&t->part_buf, need, s) != cudaSuccess) {
+        cudaGetLastError();
         t->part_buf = nullptr;
-        t->part_bytes = 0;
-        if (cudaMalloc(&t->part_buf, need) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        t->part_bytes = need;
+        return false;
     }
+    t->part_bytes = need;
+    return true;
+}
+
+bool region_sort(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t s)
+{
+    const uint64_t n = a.n;
+    region_plan pl;
+    if (!plan_regions(t, n, pl)) return false;
+    if (!grow_scratch(t, pl.need, s)) return false;
+    const uint32_t shift = pl.shift, R = pl.R;
+    const uint64_t cap = pl.cap, nv = pl.nv, cur_off = pl.cur_off, ovf_off = pl.ovf_off;
     unsigned char *p = static_cast<unsigned char *>(t->part_buf);
     uint64_t *okeys = reinterpret_cast<uint64_t *>(p);
     void *ovals = a.vals_in ? static_cast<void *>(p + nv * 8) : nullptr;
@@ -282,6 +309,13 @@ bool region_sort(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t 
 }
 
 }  // namespace
+
+bool pg_partition_reserve(pg_table *t, uint64_t max_keys, cudaStream_t s)
+{
+    region_plan pl;
+    if (!plan_regions(t, max_keys, pl)) return true;  // such batches take the ordinary path: nothing to reserve
+    return grow_scratch(t, pl.need, s);
+}
 
 bool pg_partition_insert(pg_table *t, bulk_args &a, const uint32_t *&only, cudaStream_t s)
 {

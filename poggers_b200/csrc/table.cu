@@ -396,6 +396,12 @@ pg_status pg_table_set_partitioned_insert(pg_table *t, int enable)
     return PG_OK;
 }
 
+pg_status pg_table_reserve_insert_scratch(pg_table *t, uint64_t max_batch_keys, pg_stream_t stream)
+{
+    if (!t) return PG_ERR_INVALID;
+    return pg_partition_reserve(t, max_batch_keys, reinterpret_cast<cudaStream_t>(stream)) ? PG_OK : PG_ERR_NOMEM;
+}
+
 pg_status pg_table_set_launch(pg_table *t, uint32_t block_threads, uint32_t blocks_per_sm, uint32_t max_blocks,
                               uint32_t lanes_per_key)
 {

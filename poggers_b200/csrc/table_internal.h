@@ -31,3 +31,5 @@ namespace pg { struct bulk_args; }
 // Region-ordered insert (partition.cu): true when it rewrote `a` to the sorted
 // copy; `only` then marks the keys of the caller's batch left for a second pass.
 bool pg_partition_insert(pg_table *t, pg::bulk_args &a, const uint32_t *&only, cudaStream_t s);
+// Grow that scratch for batches of up to max_keys (stream-ordered); false if it cannot be allocated.
+bool pg_partition_reserve(pg_table *t, uint64_t max_keys, cudaStream_t s);

@@ -163,3 +163,26 @@ def test_ordered_insert_with_a_full_run(pg):
     # the copies fill the key's 20 buckets (160 slots) but for the distinct keys
     # that concurrent placement put there first, which differs between the runs
     assert all(100 <= p <= 160 for p in placed) and abs(placed[0] - placed[1]) <= 32, placed
+
+
+def test_reserved_scratch_means_no_allocation_in_the_insert(pg):
+    """pg_table_reserve_insert_scratch grows the region sort's scratch ahead
+    of time: a region-ordered insert of that size then adds nothing to the
+    table's device bytes, and every key is found with its value."""
+    import torch
+    from tests.gpu_util import Driver
+    cfg = pg.data_structs.hash_table_64(1 << 23, bucket=8)
+    cfg.fingerprints = True
+    t = pg.Table(cfg, 12)
+    n = 1 << 21
+    before = t.host_bytes_in_use()
+    t.reserve_insert_scratch(n)
+    torch.cuda.synchronize()
+    reserved = t.host_bytes_in_use()
+    assert reserved > before
+    keys = wl.keys_without_sentinels(13, n)
+    vals = wl.values_for(keys, 8, 14)
+    ok = Driver(t).insert(keys, vals)
+    assert t.host_bytes_in_use() == reserved and ok.all()
+    f, v = Driver(t).query(keys)
+    assert f.all() and (v == vals).all()
