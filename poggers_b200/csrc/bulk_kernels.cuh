@@ -51,6 +51,12 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 // The fingerprint walk is latency-bound on L2 round trips: full occupancy (8
 // blocks of 256, 32 registers) measured 7 % faster on the region-ordered
 // insert at 2^26 slots despite a few bytes of spill.
+#ifndef PG_INSERT_LDCS
+#define PG_INSERT_LDCS 0
+#endif
+#ifndef PG_FP_MIN_BLOCKS
+#define PG_FP_MIN_BLOCKS 8
+#endif
 // The filters' kernels (16-bit tags) are bound by random sector reads and
 // need many keys in flight: held to 6 resident blocks of 256 (40 registers,
 // a few spilled words) they ran 1.2-1.4x faster than at their natural 93-103
@@ -64,7 +70,7 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 template <int FMT, int G = 1>
 constexpr int min_blocks_of()
 {
-    if (FMT == FMT_KV64_FP) return 8;
+    if (FMT == FMT_KV64_FP) return PG_FP_MIN_BLOCKS;
     if ((FMT == FMT_TAGVAL16 || FMT == FMT_TAGVAL16_SPLIT || FMT == FMT_TAG16) && G == 1) return PG_FILTER_MIN_BLOCKS;
     return PG_MIN_BLOCKS;
 }
@@ -109,10 +115,18 @@ __global__ void __launch_bounds__(256, min_blocks_of<FMT, G>()) k_bulk(table_des
                 if (i - r * a.region_cap >= a.region_cursor[r] - r * a.region_cap) continue;
             }
         }
+#if PG_INSERT_LDCS
+        const uint64_t key = OP == OP_INSERT ? __ldcs(a.keys + i) : __ldg(a.keys + i);
+#else
         const uint64_t key = __ldg(a.keys + i);
+#endif
         bool r;
         if constexpr (OP == OP_INSERT) {
+#if PG_INSERT_LDCS
+            V v = vin ? __ldcs(vin + i) : (V)0;
+#else
             V v = vin ? __ldg(vin + i) : (V)0;
+#endif
             r = T::insert(t, g, key, v);
             if (g.gl == 0) {
                 if (a.flags) {

@@ -18,14 +18,25 @@ struct packed_args {
     uint64_t n;
 };
 
-// build knob: resident blocks the register allocation must allow; 1 measured
-// fastest on the delete flow at 2^28 slots (5: -3.5 %, 6: -7 %, from spills)
-#ifndef PG_PACKED_MIN_BLOCKS
-#define PG_PACKED_MIN_BLOCKS 1
+// Resident blocks of 256 the register allocation must allow.  Held to 6
+// (40 registers, a few words spilled) the kernels keep 1.5x the keys in flight
+// of their natural 62-64 registers (4 blocks); measured on the delete flow
+// (insert, remove, query, re-add):
+//   4 lanes: held 1.33x and 1.35x faster at 2^24 and 2^28 slots;
+//   1 lane:  held 1.10x, 1.14x, 1.05x faster at 2^24, 2^25, 2^26 slots (64 to
+//            256 MiB, much of it in L2), 0.93x at 2^27 and 2^28 (0.5 and
+//            1 GiB: random DRAM sector reads bound them, and the spilled
+//            words only add traffic).
+// So the one-lane kernels are built both ways and chosen per launch by the
+// primary level's bytes.
+constexpr int kPackedHeldBlocks = 6;
+#ifndef PG_PACKED_HELD_MAX_MB
+#define PG_PACKED_HELD_MAX_MB 256
 #endif
+constexpr uint64_t kPackedHeldMaxBytes = (uint64_t)PG_PACKED_HELD_MAX_MB << 20;
 
-template <int W, int B0, int B1, int G, bool BK, int OP>
-__global__ void __launch_bounds__(256, PG_PACKED_MIN_BLOCKS) k_bulk_packed(table_desc t, packed_args a)
+template <int W, int B0, int B1, int G, bool BK, int OP, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_bulk_packed(table_desc t, packed_args a)
 {
     using T = packed_table<W, B0, B1, G, BK>;
     using V = typename pk<W>::V;
@@ -53,21 +64,35 @@ __global__ void __launch_bounds__(256, PG_PACKED_MIN_BLOCKS) k_bulk_packed(table
     add_count(a.count, c);
 }
 
+template <int W, int B0, int B1, int G, bool BK, int MINB>
+cudaError_t launch_packed_minb(int op, const table_desc &t, const packed_args &a, dim3 grid, dim3 block,
+                               cudaStream_t s)
+{
+    switch (op) {
+    case POP_INSERT: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT, MINB><<<grid, block, 0, s>>>(t, a); break;
+    case POP_QUERY: k_bulk_packed<W, B0, B1, G, BK, POP_QUERY, MINB><<<grid, block, 0, s>>>(t, a); break;
+    case POP_REMOVE: k_bulk_packed<W, B0, B1, G, BK, POP_REMOVE, MINB><<<grid, block, 0, s>>>(t, a); break;
+    case POP_INSERT_DELETE: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_DELETE, MINB><<<grid, block, 0, s>>>(t, a); break;
+    case POP_INSERT_IF_NOT_EXISTS:
+        k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_IF_NOT_EXISTS, MINB><<<grid, block, 0, s>>>(t, a);
+        break;
+    default: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_IF_NOT_EXISTS_DELETE, MINB><<<grid, block, 0, s>>>(t, a); break;
+    }
+    return cudaGetLastError();
+}
+
 template <int W, int B0, int B1, int G, bool BK>
 cudaError_t launch_packed_op(int op, const table_desc &t, const packed_args &a, dim3 grid, dim3 block,
                              cudaStream_t s)
 {
-    switch (op) {
-    case POP_INSERT: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT><<<grid, block, 0, s>>>(t, a); break;
-    case POP_QUERY: k_bulk_packed<W, B0, B1, G, BK, POP_QUERY><<<grid, block, 0, s>>>(t, a); break;
-    case POP_REMOVE: k_bulk_packed<W, B0, B1, G, BK, POP_REMOVE><<<grid, block, 0, s>>>(t, a); break;
-    case POP_INSERT_DELETE: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_DELETE><<<grid, block, 0, s>>>(t, a); break;
-    case POP_INSERT_IF_NOT_EXISTS:
-        k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_IF_NOT_EXISTS><<<grid, block, 0, s>>>(t, a);
-        break;
-    default: k_bulk_packed<W, B0, B1, G, BK, POP_INSERT_IF_NOT_EXISTS_DELETE><<<grid, block, 0, s>>>(t, a); break;
+    if constexpr (G > 1) {
+        return launch_packed_minb<W, B0, B1, G, BK, kPackedHeldBlocks>(op, t, a, grid, block, s);
+    } else {
+        const uint64_t bytes = t.lv[0].nbmod.d * (uint64_t)t.lv[0].bucket_bytes;
+        if (bytes <= kPackedHeldMaxBytes)
+            return launch_packed_minb<W, B0, B1, G, BK, kPackedHeldBlocks>(op, t, a, grid, block, s);
+        return launch_packed_minb<W, B0, B1, G, BK, 1>(op, t, a, grid, block, s);
     }
-    return cudaGetLastError();
 }
 
 // backing bucket: 8 or 16 slots (the reference's backing tables use 8)

@@ -251,6 +251,9 @@ __global__ void __launch_bounds__(256) k_rebuild_fp(const unsigned char *base, u
 uint32_t pg_table_lanes(const pg_table *t, int op)
 {
     if (t->ifmt == FMT_PACKED16 || t->ifmt == FMT_PACKED8) return t->lanes >= 4 ? 4u : 1u;  // compiled widths
+    // the fingerprinted kernels serve one key per lane: a grid sized for more
+    // lanes per key would launch blocks past the batch's end
+    if (t->ifmt == FMT_KV64_FP) return 1u;
     if (t->lanes) return t->lanes;
     const pg_level_config &L0 = t->cfg.levels[0];
     if (op == OP_INSERT && L0.scheme == PG_SCHEME_TWO_CHOICE && L0.nslots < (1ull << 18) &&
