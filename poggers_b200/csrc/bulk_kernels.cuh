@@ -50,10 +50,8 @@ __device__ __forceinline__ void add_count(unsigned long long *count, uint32_t c)
 
 // The fingerprint walk is latency-bound on L2 round trips: full occupancy (8
 // blocks of 256, 32 registers) measured 7 % faster on the region-ordered
-// insert at 2^26 slots despite a few bytes of spill.
-#ifndef PG_INSERT_LDCS
-#define PG_INSERT_LDCS 0
-#endif
+// insert at 2^26 slots despite a few bytes of spill (and 6 blocks, 40
+// registers, 6 % slower on the insert kernel again after later changes).
 #ifndef PG_FP_MIN_BLOCKS
 #define PG_FP_MIN_BLOCKS 8
 #endif
@@ -115,18 +113,10 @@ __global__ void __launch_bounds__(256, min_blocks_of<FMT, G>()) k_bulk(table_des
                 if (i - r * a.region_cap >= a.region_cursor[r] - r * a.region_cap) continue;
             }
         }
-#if PG_INSERT_LDCS
-        const uint64_t key = OP == OP_INSERT ? __ldcs(a.keys + i) : __ldg(a.keys + i);
-#else
         const uint64_t key = __ldg(a.keys + i);
-#endif
         bool r;
         if constexpr (OP == OP_INSERT) {
-#if PG_INSERT_LDCS
-            V v = vin ? __ldcs(vin + i) : (V)0;
-#else
             V v = vin ? __ldg(vin + i) : (V)0;
-#endif
             r = T::insert(t, g, key, v);
             if (g.gl == 0) {
                 if (a.flags) {
