@@ -12,6 +12,9 @@
  *    (NULL = the legacy default stream).  Calls on the same table must be
  *    phase-separated by stream order: the reference's guarantee that a query
  *    sees an insert holds only across kernel boundaries, and so does ours.
+ *  - Tables, batches, servers and allocators live on the device current when
+ *    they are created; every later call on one must be made with that device
+ *    current, or it returns PG_ERR_INVALID and launches nothing.
  *  - Errors are status codes, never exceptions or device traps.  The
  *    reference throws std::runtime_error on a sizing mismatch
  *    (tables/base_table.cuh:116-131) and returns bool from device ops.
@@ -323,9 +326,8 @@ pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_n
  * library, at most PG_STATIC_MAX_TABLES tables and PG_STATIC_MAX_OPS requests
  * per call (larger calls return PG_ERR_TOO_LARGE).  That array (about 106 KB)
  * exists once on every GPU that loads the library, until the process exits.
- *  - The first call on a device looks up the array's device address; make that
- *    first call before capturing a stream into a CUDA graph.  The address is
- *    kept for the process's life, so do not use the call across a
+ *  - The first call on a device looks up the array's device address and keeps
+ *    it for the process's life, so do not use the call across a
  *    cudaDeviceReset().
  *  - The current device must be the tables' device (else PG_ERR_INVALID,
  *    before anything is launched).

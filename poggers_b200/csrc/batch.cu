@@ -28,6 +28,7 @@ struct pg_batch {
     unsigned long long clear_padded;
     unsigned long long *d_scratch;  // chunk_start[max_ops + 1] then the work counter
     int num_sms;
+    int device;  // the tables' device
     uint32_t block_threads, blocks_per_sm, lanes;
 };
 
@@ -205,6 +206,7 @@ pg_status pg_batch_create(pg_table *const *tables, uint32_t ntables, uint32_t ma
     b->backing = t0->cfg.nlevels > 1;
     b->bucket1 = backing_bucket(t0);
     b->num_sms = t0->num_sms;
+    b->device = t0->device;
     b->block_threads = 256;
     b->blocks_per_sm = 8;
     b->lanes = pg_table_lanes(t0);
@@ -266,7 +268,7 @@ pg_status pg_batch_destroy(pg_batch *b)
 
 pg_status pg_batch_clear(pg_batch *b, pg_stream_t stream)
 {
-    if (!b) return PG_ERR_INVALID;
+    if (!b || !pg_on_device(b->device)) return PG_ERR_INVALID;
     if (b->nseg == 0) return PG_OK;
     const unsigned long long chunks = b->clear_padded / 16;
     unsigned long long blocks = (chunks + 255) / 256;
@@ -300,7 +302,7 @@ pg_status pg_batch_run(pg_batch *b, const pg_op_desc *d_ops, const uint32_t *d_n
                        const void *d_vals_in, void *d_vals_out, uint8_t *d_flags, uint64_t *d_op_counts,
                        pg_stream_t stream)
 {
-    if (!b || !d_ops || !d_nops || !d_keys) return PG_ERR_INVALID;
+    if (!b || !d_ops || !d_nops || !d_keys || !pg_on_device(b->device)) return PG_ERR_INVALID;
     batch_args a;
     a.tables = b->d_tables;
     a.ops = d_ops;

@@ -586,7 +586,8 @@ pg_status pg_server_destroy(pg_server *s)
 
 pg_status pg_server_add_table(pg_server *s, const pg_table_config *cfg, uint64_t seed, uint32_t *table_id)
 {
-    if (!s || !cfg || !table_id) return PG_ERR_INVALID;
+    // the table is created on the current device, which must be the server's
+    if (!s || !cfg || !table_id || !pg_on_device(s->device)) return PG_ERR_INVALID;
     // admission by HBM budget: the table's slot arrays (and fingerprints) must fit
     uint64_t need = 0;
     const uint32_t kb = cfg->format == PG_FMT_KV64 ? 8 : cfg->format == PG_FMT_PACKED_TAGVAL8 ? 1 : 2;
@@ -707,7 +708,8 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
 pg_status pg_server_add_slab_set(pg_server *s, uint32_t nclasses, const uint64_t *class_bytes,
                                  const uint64_t *num_allocs, uint32_t *set_id)
 {
-    if (!s || !class_bytes || !num_allocs || !set_id || nclasses == 0) return PG_ERR_INVALID;
+    if (!s || !class_bytes || !num_allocs || !set_id || nclasses == 0 || !pg_on_device(s->device))
+        return PG_ERR_INVALID;
     // admission: every class's pool (whole slabs of 4096 objects) and its bitmaps
     uint64_t need = 0;
     for (uint32_t c = 0; c < nclasses; c++) {

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "poggers_b200.h"
+#include "on_device.h"
 #include "poggers_b200/slab.cuh"
 
 using namespace pg;
@@ -15,6 +16,7 @@ struct pg_slab {
     uint64_t capacity;
     uint64_t pool_bytes;
     int device;
+    int num_sms;
 };
 
 struct pg_slab_set {
@@ -148,9 +150,11 @@ pg_status pg_slab_create(uint64_t num_allocs, uint64_t object_bytes, pg_slab **o
     *out = nullptr;
     pg_slab *a = (pg_slab *)calloc(1, sizeof(pg_slab));
     if (!a) return PG_ERR_NOMEM;
-    cudaGetDevice(&a->device);
     const uint64_t nslabs = (num_allocs - 1) / kSlabObjects + 1;  // slab_one_size.cuh:94
-    if (nslabs > 0xFFFFFFFEull) {
+    if (nslabs > 0xFFFFFFFEull || object_bytes > ~0ull / (nslabs * kSlabObjects) ||
+        cudaGetDevice(&a->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&a->num_sms, cudaDevAttrMultiProcessorCount, a->device) != cudaSuccess) {
+        cudaGetLastError();
         free(a);
         return PG_ERR_INVALID;
     }
@@ -201,7 +205,7 @@ pg_status pg_slab_destroy(pg_slab *a)
 
 pg_status pg_slab_reset(pg_slab *a, pg_stream_t stream)
 {
-    if (!a) return PG_ERR_INVALID;
+    if (!a || !pg_on_device(a->device)) return PG_ERR_INVALID;
     const uint64_t words = a->d.nslabs * kSlabWords;
     uint64_t blocks = (words + 255) / 256;
     if (blocks > 4096) blocks = 4096;
@@ -223,7 +227,7 @@ pg_status pg_slab_info(const pg_slab *a, pg_slab_info_t *out)
 
 pg_status pg_slab_bulk_malloc(pg_slab *a, uint64_t n, void **d_ptrs, uint64_t *d_fail_count, pg_stream_t stream)
 {
-    if (!a || (n && !d_ptrs)) return PG_ERR_INVALID;
+    if (!a || (n && !d_ptrs) || !pg_on_device(a->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     k_slab_malloc<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, n, d_ptrs, reinterpret_cast<unsigned long long *>(d_fail_count));
@@ -239,10 +243,10 @@ pg_status pg_slab_desc(const pg_slab *a, void *out_desc, uint64_t bytes)
 
 pg_status pg_slab_bulk_free(pg_slab *a, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count, pg_stream_t stream)
 {
-    if (!a || (n && !d_ptrs)) return PG_ERR_INVALID;
+    if (!a || (n && !d_ptrs) || !pg_on_device(a->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     uint64_t blocks = grid_for(n);
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks > (uint64_t)a->num_sms * 32) blocks = (uint64_t)a->num_sms * 32;
     k_slab_free<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, n, d_ptrs, reinterpret_cast<unsigned long long *>(d_bad_count));
     return cuda_status(cudaGetLastError());
@@ -250,9 +254,9 @@ pg_status pg_slab_bulk_free(pg_slab *a, void *const *d_ptrs, uint64_t n, uint64_
 
 pg_status pg_slab_count_free(pg_slab *a, uint64_t *d_out, pg_stream_t stream)
 {
-    if (!a || !d_out) return PG_ERR_INVALID;
+    if (!a || !d_out || !pg_on_device(a->device)) return PG_ERR_INVALID;
     uint64_t blocks = (a->d.nslabs + 255) / 256;
-    if (blocks > 1184) blocks = 1184;
+    if (blocks > (uint64_t)a->num_sms * 8) blocks = (uint64_t)a->num_sms * 8;
     k_slab_count<<<(unsigned)(blocks ? blocks : 1), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, reinterpret_cast<unsigned long long *>(d_out));
     return cuda_status(cudaGetLastError());
@@ -261,11 +265,11 @@ pg_status pg_slab_count_free(pg_slab *a, uint64_t *d_out, pg_stream_t stream)
 pg_status pg_slab_report(pg_slab *a, uint64_t *free_slabs, uint64_t *max_slabs, uint64_t *free_objects,
                          uint64_t *double_frees)
 {
-    if (!a) return PG_ERR_INVALID;
+    if (!a || !pg_on_device(a->device)) return PG_ERR_INVALID;
     unsigned long long *d = nullptr;
     if (cudaMalloc(&d, 16) != cudaSuccess) return PG_ERR_NOMEM;
-    cudaMemset(d, 0, 16);
-    pg_status st = pg_slab_count_free(a, reinterpret_cast<uint64_t *>(d), nullptr);
+    pg_status st = cuda_status(cudaMemset(d, 0, 16));
+    if (st == PG_OK) st = pg_slab_count_free(a, reinterpret_cast<uint64_t *>(d), nullptr);
     unsigned long long h[2] = {0, 0}, s[2] = {0, 0};
     if (st == PG_OK) st = cuda_status(cudaMemcpy(h, d, 16, cudaMemcpyDeviceToHost));
     if (st == PG_OK) st = cuda_status(cudaMemcpy(s, a->d.stats, 16, cudaMemcpyDeviceToHost));
@@ -327,7 +331,7 @@ static set_desc make_set(const pg_slab_set *s)
 pg_status pg_slab_set_bulk_malloc(pg_slab_set *s, const uint32_t *d_sizes, uint64_t n, void **d_ptrs,
                                   uint64_t *d_fail_count, pg_stream_t stream)
 {
-    if (!s || (n && (!d_ptrs || !d_sizes))) return PG_ERR_INVALID;
+    if (!s || (n && (!d_ptrs || !d_sizes)) || !pg_on_device(s->cls[0]->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     k_set_malloc<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         make_set(s), n, d_sizes, d_ptrs, reinterpret_cast<unsigned long long *>(d_fail_count));
@@ -337,10 +341,10 @@ pg_status pg_slab_set_bulk_malloc(pg_slab_set *s, const uint32_t *d_sizes, uint6
 pg_status pg_slab_set_bulk_free(pg_slab_set *s, void *const *d_ptrs, uint64_t n, uint64_t *d_bad_count,
                                 pg_stream_t stream)
 {
-    if (!s || (n && !d_ptrs)) return PG_ERR_INVALID;
+    if (!s || (n && !d_ptrs) || !pg_on_device(s->cls[0]->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     uint64_t blocks = grid_for(n);
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks > (uint64_t)s->cls[0]->num_sms * 32) blocks = (uint64_t)s->cls[0]->num_sms * 32;
     k_set_free<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         make_set(s), n, d_ptrs, reinterpret_cast<unsigned long long *>(d_bad_count));
     return cuda_status(cudaGetLastError());

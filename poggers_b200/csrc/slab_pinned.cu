@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "poggers_b200.h"
+#include "on_device.h"
 #include "poggers_b200/slab_pinned.cuh"
 
 using namespace pg;
@@ -128,10 +129,15 @@ pg_status pg_pslab_create(uint64_t num_allocs, uint64_t object_bytes, uint32_t e
 {
     if (!out || num_allocs == 0 || object_bytes == 0 || extra_blocks + 1 >= kPinnedPlaces) return PG_ERR_INVALID;
     *out = nullptr;
+    const uint64_t nslabs = (num_allocs - 1) / kPinnedObjects + 1;  // slab_one_size.cuh:94
+    if (nslabs > 0xFFFFFFFEull || object_bytes > ~0ull / (nslabs * kPinnedObjects)) return PG_ERR_INVALID;
     pg_pslab *a = (pg_pslab *)calloc(1, sizeof(pg_pslab));
     if (!a) return PG_ERR_NOMEM;
-    cudaGetDevice(&a->device);
-    const uint64_t nslabs = (num_allocs - 1) / kPinnedObjects + 1;  // slab_one_size.cuh:94
+    if (cudaGetDevice(&a->device) != cudaSuccess) {
+        cudaGetLastError();
+        free(a);
+        return PG_ERR_CUDA;
+    }
     a->d.nslabs = nslabs;
     a->d.size = object_bytes;
     a->d.extra = extra_blocks;
@@ -200,7 +206,7 @@ pg_status pg_pslab_desc(const pg_pslab *a, void *out_desc, uint64_t bytes)
 pg_status pg_pslab_report(const pg_pslab *a, uint64_t *pool_slabs, uint64_t *max_slabs, uint64_t *sm_ids,
                           uint64_t *double_frees)
 {
-    if (!a) return PG_ERR_INVALID;
+    if (!a || !pg_on_device(a->device)) return PG_ERR_INVALID;
     const uint64_t nw = (a->d.nslabs + 63) / 64;
     std::vector<unsigned long long> h(nw);
     unsigned long long st[3] = {0, 0, 0};
@@ -217,7 +223,7 @@ pg_status pg_pslab_report(const pg_pslab *a, uint64_t *pool_slabs, uint64_t *max
 
 pg_status pg_pslab_bulk_malloc(pg_pslab *a, uint64_t n, void **d_ptrs, uint64_t *d_fail_count, pg_stream_t stream)
 {
-    if (!a || (n && !d_ptrs)) return PG_ERR_INVALID;
+    if (!a || (n && !d_ptrs) || !pg_on_device(a->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     k_pslab_malloc<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, n, d_ptrs, reinterpret_cast<unsigned long long *>(d_fail_count));
@@ -227,7 +233,7 @@ pg_status pg_pslab_bulk_malloc(pg_pslab *a, uint64_t n, void **d_ptrs, uint64_t 
 pg_status pg_pslab_serial_malloc(pg_pslab *a, uint32_t rounds, uint32_t group, void **d_ptrs, uint64_t *d_fail_count,
                                  pg_stream_t stream)
 {
-    if (!a || !d_ptrs || group == 0 || group > 32) return PG_ERR_INVALID;
+    if (!a || !d_ptrs || group == 0 || group > 32 || !pg_on_device(a->device)) return PG_ERR_INVALID;
     if (rounds == 0) return PG_OK;
     k_pslab_serial_malloc<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, rounds, group, d_ptrs, reinterpret_cast<unsigned long long *>(d_fail_count));
@@ -237,10 +243,10 @@ pg_status pg_pslab_serial_malloc(pg_pslab *a, uint32_t rounds, uint32_t group, v
 pg_status pg_pslab_bulk_free(pg_pslab *a, void *const *d_ptrs, uint64_t n, uint64_t *d_counts, int serial,
                              pg_stream_t stream)
 {
-    if (!a || !d_counts || (n && !d_ptrs)) return PG_ERR_INVALID;
+    if (!a || !d_counts || (n && !d_ptrs) || !pg_on_device(a->device)) return PG_ERR_INVALID;
     if (n == 0) return PG_OK;
     unsigned blocks = serial ? 1u : grid_for(n);
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks > a->d.nsm * 32u) blocks = a->d.nsm * 32u;  // grid-stride; %nsmid >= the SM count
     k_pslab_free<<<blocks, serial ? 32 : 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         a->d, n, d_ptrs, reinterpret_cast<unsigned long long *>(d_counts), serial ? 1u : 0u);
     return cuda_status(cudaGetLastError());

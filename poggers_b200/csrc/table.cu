@@ -127,7 +127,7 @@ void launch_shape(const pg_table *t, uint32_t lanes, uint64_t n, dim3 &grid, dim
 
 pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
 {
-    if (!t) return PG_ERR_INVALID;
+    if (!t || !pg_on_device(t->device)) return PG_ERR_INVALID;
     if (a.n == 0) return PG_OK;
     if (!a.keys) return PG_ERR_INVALID;
     dim3 grid, block;
@@ -151,7 +151,7 @@ pg_status run_bulk(pg_table *t, int op, const bulk_args &a, pg_stream_t stream)
 // the bucketed filter's operations (packed formats)
 pg_status run_packed(pg_table *t, int op, const packed_args &a, pg_stream_t stream)
 {
-    if (!t) return PG_ERR_INVALID;
+    if (!t || !pg_on_device(t->device)) return PG_ERR_INVALID;
     if (t->ifmt != FMT_PACKED16 && t->ifmt != FMT_PACKED8) return PG_ERR_UNSUPPORTED;
     if (a.n == 0) return PG_OK;
     if (!a.keys) return PG_ERR_INVALID;
@@ -365,7 +365,7 @@ pg_status pg_table_destroy(pg_table *t)
 
 pg_status pg_table_clear(pg_table *t, pg_stream_t stream)
 {
-    if (!t) return PG_ERR_INVALID;
+    if (!t || !pg_on_device(t->device)) return PG_ERR_INVALID;
     for (uint32_t l = 0; l < t->cfg.nlevels; l++) {
         cudaError_t e = cudaMemsetAsync(t->mem[l], 0, t->bytes[l], reinterpret_cast<cudaStream_t>(stream));
         if (e != cudaSuccess) return cuda_status(e);
@@ -401,7 +401,7 @@ pg_status pg_table_set_partitioned_insert(pg_table *t, int enable)
 
 pg_status pg_table_reserve_insert_scratch(pg_table *t, uint64_t max_batch_keys, pg_stream_t stream)
 {
-    if (!t) return PG_ERR_INVALID;
+    if (!t || !pg_on_device(t->device)) return PG_ERR_INVALID;
     return pg_partition_reserve(t, max_batch_keys, reinterpret_cast<cudaStream_t>(stream)) ? PG_OK : PG_ERR_NOMEM;
 }
 
@@ -431,6 +431,7 @@ pg_status pg_bulk_insert(pg_table *t, const uint64_t *d_keys, const void *d_vals
         packed_args p{d_keys, d_vals, nullptr, d_ok, nullptr, reinterpret_cast<unsigned long long *>(d_fail_count), n};
         return run_packed(t, POP_INSERT, p, stream);
     }
+    if (t && !pg_on_device(t->device)) return PG_ERR_INVALID;  // before the region sort launches anything
     bulk_args a{d_keys, t && t->cfg.format != PG_FMT_TAG16 ? d_vals : nullptr, nullptr, d_ok,
                 reinterpret_cast<unsigned long long *>(d_fail_count), n};
     const bulk_args batch = a;
@@ -494,7 +495,7 @@ pg_status pg_bulk_insert_if_not_exists_delete(pg_table *t, const uint64_t *d_key
 
 pg_status pg_table_count_fill(pg_table *t, uint32_t level, uint64_t *d_out, pg_stream_t stream)
 {
-    if (!t || !d_out || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    if (!t || !d_out || level >= t->cfg.nlevels || !pg_on_device(t->device)) return PG_ERR_INVALID;
     const level_desc &D = t->desc.lv[level];
     const uint64_t nb = D.nbmod.d;
     uint64_t blocks = (nb + 255) / 256;

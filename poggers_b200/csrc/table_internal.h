@@ -4,6 +4,7 @@
 #include "poggers_b200.h"
 #include "poggers_b200/level.cuh"
 #include <cuda_runtime.h>
+#include "on_device.h"
 
 struct pg_table {
     pg_table_config cfg;
