@@ -374,7 +374,8 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
                            uint64_t n, void *h_vals_out, uint8_t *h_flags, uint64_t *request_id);
 /* Collect a finished request: PG_OK (count = hits or failures, latency in
  * seconds from submit to completion), or PG_ERR_TIMEOUT if it is still
- * running and wait == 0.  A request is collected once. */
+ * running and wait == 0.  A request is collected once; an id that was never
+ * issued or was already collected returns PG_ERR_INVALID (it does not wait). */
 pg_status pg_server_poll(pg_server *s, uint64_t request_id, int wait, uint64_t *count, double *latency_s);
 /* Slab size-class sets served by the loop (as pg_slab_set_create; their pools
  * count against the HBM budget, PG_ERR_FULL when they would not fit).

@@ -32,6 +32,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <system_error>
 #include <thread>
 #include <vector>
@@ -107,6 +108,7 @@ struct pg_server {
     std::vector<slab_entry> slabs;
     std::deque<request *> pending;
     std::map<uint64_t, request *> done;
+    std::set<uint64_t> outstanding;  // submitted and not yet collected by pg_server_poll
     // staging (per wave slot): pinned host and device buffers
     struct stage {
         uint64_t *h_keys, *d_keys;
@@ -700,6 +702,7 @@ pg_status pg_server_submit(pg_server *s, uint32_t table_id, uint32_t op, const u
     r->t_submit = now_s();
     r->t_done = 0;
     s->pending.push_back(r);
+    s->outstanding.insert(r->id);
     *request_id = r->id;
     s->cv.notify_all();
     return PG_OK;
@@ -756,6 +759,7 @@ pg_status pg_server_submit_slab(pg_server *s, uint32_t set_id, uint32_t op, cons
     r->t_submit = now_s();
     r->t_done = 0;
     s->pending.push_back(r);
+    s->outstanding.insert(r->id);
     *request_id = r->id;
     s->cv.notify_all();
     return PG_OK;
@@ -773,8 +777,11 @@ pg_status pg_server_poll(pg_server *s, uint64_t request_id, int wait, uint64_t *
             if (latency_s) *latency_s = r->t_done - r->t_submit;
             delete r;
             s->done.erase(it);
+            s->outstanding.erase(request_id);
             return PG_OK;
         }
+        // never issued, or already collected: nothing will complete it
+        if (!s->outstanding.count(request_id)) return PG_ERR_INVALID;
         if (s->error != PG_OK) return s->error;
         if (!wait) return PG_ERR_TIMEOUT;  // not finished yet
         s->cv.wait_for(lk, std::chrono::milliseconds(1));

@@ -141,6 +141,10 @@ def test_server_admits_tables_by_hbm_budget(pg):
     f = np.zeros(100, dtype=np.uint8)
     r = srv.submit(0, 0, k, wl.values_for(k, 8, 1), None, f)
     assert srv.poll(r, wait=True)[0] == 0 and f.all()
+    # a collected id, or one never issued, is refused instead of waited on
+    for bad in (r, r + 1000):
+        with pytest.raises(pg.PoggersError):
+            srv.poll(bad, wait=True)
     srv.close()
 
 
