@@ -19,15 +19,23 @@ namespace pg {
 // Each step reads the fingerprint words of two consecutive probes of a key:
 // an absent key walks about 2.9 buckets at 0.9 load, so its chain of
 // dependent L2 round trips halves.  Measured at 2^26 slots: query 2.041 ms
-// against 2.078 reading one bucket per step (45 registers against 32; held to
-// 32, 2.260 ms).
+// against 2.078 reading one bucket per step (45 registers against 32).
 #ifndef PG_FP_QUERY_TWO_BUCKETS
 #define PG_FP_QUERY_TWO_BUCKETS 1
 #endif
 constexpr bool kTwoBuckets = PG_FP_QUERY_TWO_BUCKETS != 0;
 
+// Held to 6 resident blocks of 256 (40 registers, a word spilled) the kernel
+// ran 1.913 ms against 2.030 at its natural 46 registers (5 blocks) at 2^26
+// slots; 8 blocks (32 registers) 2.26 ms.  Dealing each block's range to its
+// warps in 128-key chunks from a shared counter (so that no warp idles at the
+// end of a fixed range) measured 1.934 ms at 6 blocks: not kept.
+#ifndef PG_FP_QUERY_MIN_BLOCKS
+#define PG_FP_QUERY_MIN_BLOCKS 6
+#endif
+
 template <int B, bool BK>
-__global__ void __launch_bounds__(256) k_query_fp_refill(table_desc t, bulk_args a)
+__global__ void __launch_bounds__(256, PG_FP_QUERY_MIN_BLOCKS) k_query_fp_refill(table_desc t, bulk_args a)
 {
     using P = level_ops_fp<B>;
     using BKO = backing_ops<FMT_KV64, 1>;
