@@ -16,26 +16,32 @@ namespace pg {
 // (first fingerprint match at or before the first empty slot of a bucket,
 // a bucket with an empty slot ends the walk); a primary miss goes to the
 // backing level.
-// Each step reads the fingerprint words of two consecutive probes of a key:
-// an absent key walks about 2.9 buckets at 0.9 load, so its chain of
-// dependent L2 round trips halves.  Measured at 2^26 slots: query 2.041 ms
-// against 2.078 reading one bucket per step (45 registers against 32).
-#ifndef PG_FP_QUERY_TWO_BUCKETS
-#define PG_FP_QUERY_TWO_BUCKETS 1
+// While the fingerprint array stays in L2 (level_desc::fp_resident), each
+// step reads the fingerprint words of two consecutive probes of a key: an
+// absent key walks about 2.9 buckets at 0.9 load, so its chain of dependent
+// L2 round trips halves.  Measured at 2^26 slots: query 2.041 ms against
+// 2.078 reading one bucket per step (45 registers against 32).  A larger
+// array is read from DRAM, where the second word read is a second random
+// access for every key: at 2^30 slots (1 GiB of fingerprints) the query
+// took 66.2 ms reading two buckets per step against 52.6 reading one.
+// Build knob: 0 = one bucket per step always, 1 = two while resident, 2 = two always.
+#ifndef PG_FP_QUERY_TWO_MODE
+#define PG_FP_QUERY_TWO_MODE 1
 #endif
-constexpr bool kTwoBuckets = PG_FP_QUERY_TWO_BUCKETS != 0;
 
-// Held to 6 resident blocks of 256 (40 registers, a word spilled) the kernel
-// ran 1.913 ms against 2.030 at its natural 46 registers (5 blocks) at 2^26
-// slots; 8 blocks (32 registers) 2.26 ms.  Dealing each block's range to its
-// warps in 128-key chunks from a shared counter (so that no warp idles at the
-// end of a fixed range) measured 1.934 ms at 6 blocks: not kept.
+// Reading two buckets per step, held to 6 resident blocks of 256 (40
+// registers, a word spilled) the kernel ran 1.913 ms against 2.030 at its
+// natural 46 registers (5 blocks) at 2^26 slots; 8 blocks (32 registers)
+// 2.26 ms.  Dealing each block's range to its warps in 128-key chunks from a
+// shared counter (so that no warp idles at the end of a fixed range) measured
+// 1.934 ms at 6 blocks: not kept.  Reading one bucket per step it fits 32
+// registers, full occupancy.
 #ifndef PG_FP_QUERY_MIN_BLOCKS
 #define PG_FP_QUERY_MIN_BLOCKS 6
 #endif
 
-template <int B, bool BK>
-__global__ void __launch_bounds__(256, PG_FP_QUERY_MIN_BLOCKS) k_query_fp_refill(table_desc t, bulk_args a)
+template <int B, bool BK, bool TWO>
+__global__ void __launch_bounds__(256, TWO ? PG_FP_QUERY_MIN_BLOCKS : 8) k_query_fp_refill(table_desc t, bulk_args a)
 {
     using P = level_ops_fp<B>;
     using BKO = backing_ops<FMT_KV64, 1>;
@@ -72,7 +78,7 @@ __global__ void __launch_bounds__(256, PG_FP_QUERY_MIN_BLOCKS) k_query_fp_refill
         }
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
-            // one bucket of this lane's key (two with kTwoBuckets: the next
+            // one bucket of this lane's key (two with TWO: the next
             // probe's fingerprints are read with this one's and looked at only
             // if the walk goes on, so the results are the same)
             bool done = false, hit = false;
@@ -86,7 +92,7 @@ __global__ void __launch_bounds__(256, PG_FP_QUERY_MIN_BLOCKS) k_query_fp_refill
                 P::load_fp(L, b, w, keep);
                 uint64_t b2 = 0;
                 bool two = false;
-                if constexpr (kTwoBuckets) {
+                if constexpr (TWO) {
                     if (i + 1 < L.max_probes) {
                         const uint64_t raw2 = ps.at(i + 1);
                         if (raw2 != kProbeEnd) {
@@ -115,7 +121,7 @@ __global__ void __launch_bounds__(256, PG_FP_QUERY_MIN_BLOCKS) k_query_fp_refill
                 };
                 uint32_t e = look(b, w);
                 done = hit || e != 0 || ++i >= L.max_probes;
-                if (kTwoBuckets && !done && two) {
+                if (TWO && !done && two) {
                     e = look(b2, w2);
                     done = hit || e != 0 || ++i >= L.max_probes;
                 }
@@ -165,18 +171,25 @@ int refill_blocks(const void *fn)
     return sms * per_sm;
 }
 
-template <int B, bool BK>
-cudaError_t launch_query_refill(const table_desc &t, const bulk_args &a, dim3 grid, cudaStream_t s)
+template <int B, bool BK, bool TWO>
+cudaError_t launch_query_refill_k(const table_desc &t, const bulk_args &a, dim3 grid, cudaStream_t s)
 {
-    const void *fn = (const void *)k_query_fp_refill<B, BK>;
+    const void *fn = (const void *)k_query_fp_refill<B, BK, TWO>;
     const int blocks = refill_blocks(fn);
     // one resident wave of blocks, never more warps than keys
     uint64_t g = blocks > 0 ? (uint64_t)blocks : grid.x;
     const uint64_t max_by_keys = (a.n + 255) / 256;
     if (g > max_by_keys) g = max_by_keys;
     if (g < 1) g = 1;
-    k_query_fp_refill<B, BK><<<(unsigned)g, 256, 0, s>>>(t, a);
+    k_query_fp_refill<B, BK, TWO><<<(unsigned)g, 256, 0, s>>>(t, a);
     return cudaGetLastError();
+}
+
+template <int B, bool BK>
+cudaError_t launch_query_refill(const table_desc &t, const bulk_args &a, dim3 grid, cudaStream_t s)
+{
+    const bool two = PG_FP_QUERY_TWO_MODE == 2 || (PG_FP_QUERY_TWO_MODE == 1 && t.lv[0].fp_resident);
+    return two ? launch_query_refill_k<B, BK, true>(t, a, grid, s) : launch_query_refill_k<B, BK, false>(t, a, grid, s);
 }
 
 template <int B>
