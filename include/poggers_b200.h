@@ -389,6 +389,16 @@ pg_status pg_server_add_slab_set(pg_server *s, uint32_t nclasses, const uint64_t
 pg_status pg_server_submit_slab(pg_server *s, uint32_t set_id, uint32_t op, const void *h_in, uint64_t n,
                                 uint64_t *h_ptrs_out, uint64_t *request_id);
 pg_status pg_server_stats(pg_server *s, uint64_t *waves, uint64_t *keys);
+/* Where the server's worker thread spent its time since creation (seconds):
+ * planning waves (with the lock held), copying request inputs into pinned
+ * staging, issuing the wave's copies and runs, copying results out to the
+ * clients' buffers, and waiting -- with waves in flight and no free slot or
+ * nothing pending (busy), or with nothing in flight (idle). */
+typedef struct pg_server_timing_t {
+    uint64_t waves, requests, keys;
+    double plan_s, copy_in_s, issue_s, copy_out_s, wait_busy_s, wait_idle_s;
+} pg_server_timing_t;
+pg_status pg_server_timing(pg_server *s, pg_server_timing_t *out);
 
 /* ---------------------------------------------------------------------------
  * Slab allocator: fixed-size objects from slabs of 4096.

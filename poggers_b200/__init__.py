@@ -71,6 +71,12 @@ class _ServerConfig(C.Structure):
                 ("max_wave_requests", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class _ServerTiming(C.Structure):
+    _fields_ = [("waves", C.c_uint64), ("requests", C.c_uint64), ("keys", C.c_uint64),
+                ("plan_s", C.c_double), ("copy_in_s", C.c_double), ("issue_s", C.c_double),
+                ("copy_out_s", C.c_double), ("wait_busy_s", C.c_double), ("wait_idle_s", C.c_double)]
+
+
 class _SlabInfo(C.Structure):
     _fields_ = [("pool", C.c_void_p), ("pool_bytes", C.c_uint64), ("object_bytes", C.c_uint64),
                 ("capacity", C.c_uint64), ("nslabs", C.c_uint64), ("d_stats", C.c_void_p)]
@@ -95,7 +101,7 @@ EXPORTED = (
     "pg_pslab_create", "pg_pslab_destroy", "pg_pslab_desc", "pg_pslab_report", "pg_pslab_bulk_malloc",
     "pg_pslab_serial_malloc", "pg_pslab_bulk_free",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
-    "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats",
+    "pg_server_bytes_in_use", "pg_server_submit", "pg_server_poll", "pg_server_stats", "pg_server_timing",
     "pg_server_add_slab_set", "pg_server_submit_slab",
     "pg_diag_random_access",
 )
@@ -234,6 +240,8 @@ def lib() -> C.CDLL:
     L.pg_server_poll.argtypes = [V, U64, C.c_int, C.POINTER(U64), C.POINTER(C.c_double)]
     L.pg_server_stats.restype = C.c_int
     L.pg_server_stats.argtypes = [V, C.POINTER(U64), C.POINTER(U64)]
+    L.pg_server_timing.restype = C.c_int
+    L.pg_server_timing.argtypes = [V, C.POINTER(_ServerTiming)]
     L.pg_host_murmur64a.restype = U64
     L.pg_host_murmur64a.argtypes = [U64, U64]
     L.pg_host_fastmod.restype = U64
@@ -851,3 +859,9 @@ class Server:
         w, k = C.c_uint64(), C.c_uint64()
         _check(lib().pg_server_stats(self._h, C.byref(w), C.byref(k)), "pg_server_stats")
         return w.value, k.value
+
+    def timing(self) -> dict:
+        """The worker thread's time by stage since creation (pg_server_timing)."""
+        t = _ServerTiming()
+        _check(lib().pg_server_timing(self._h, C.byref(t)), "pg_server_timing")
+        return {f: getattr(t, f) for f, _ in _ServerTiming._fields_}

@@ -293,6 +293,7 @@ def config4(args):
     vals_of = [wl.values_for(k, 8 if kind == "ht" else 2, 1) if op == 0 else None for _, op, k, kind in reqs]
     results = {}
     for rate in args.rates:
+        tm0 = srv.timing()
         gaps = rng.exponential(1.0 / rate, len(reqs))
         arrive = np.cumsum(gaps)
         outs = [np.zeros(len(k), dtype=np.uint64 if kind == "ht" else np.uint16) if op == 1 else None
@@ -305,9 +306,12 @@ def config4(args):
             rids.append(srv.submit(tid, op, k, vals, vout, None))
         lats = [srv.poll(r, wait=True)[1] for r in rids]
         el = time.perf_counter() - t0
+        tm1 = srv.timing()
         results[str(rate)] = {"offered_req_s": rate, "achieved_mops": round(total_keys / el / 1e6, 1),
                               "p50_ms": round(1e3 * float(np.percentile(lats, 50)), 3),
-                              "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3)}
+                              "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3),
+                              "worker": {k: (round(tm1[k] - tm0[k], 4) if k.endswith("_s") else tm1[k] - tm0[k])
+                                         for k in tm1}}
     waves, _ = srv.stats()
     in_use = srv.bytes_in_use()
     # plain path: the same requests one launch each, in order, from host buffers

@@ -126,6 +126,9 @@ struct pg_server {
     } stages[kMaxWaves];
     uint64_t waves_run = 0;
     uint64_t keys_run = 0;
+    uint64_t requests_run = 0;
+    // the worker thread's time by stage (seconds; written with the lock held)
+    double t_plan = 0, t_copy_in = 0, t_issue = 0, t_copy_out = 0, t_wait_busy = 0, t_wait_idle = 0;
     pg_status error = PG_OK;
 };
 
@@ -217,47 +220,109 @@ struct copy_job {
     uint64_t bytes;
 };
 
-// Run the copies of one wave.  A single thread's memcpy moves a fraction of
-// what host memory and the PCIe link take, so a wave of more than 8 MB is
-// split into equal byte ranges over up to 8 threads (half the host's
-// hardware threads at most).
-void copy_all(const std::vector<copy_job> &jobs)
+// Copy one byte range [lo, hi) of the concatenated jobs.
+void copy_range(const std::vector<copy_job> &jobs, uint64_t lo, uint64_t hi)
 {
-    uint64_t total = 0;
-    for (const copy_job &j : jobs) total += j.bytes;
-    const unsigned hw = std::thread::hardware_concurrency();
-    const unsigned nt = total < (8ull << 20) ? 1u : std::max(1u, std::min(8u, hw / 2));
-    auto part = [&](unsigned k) {
-        const uint64_t lo = total * k / nt, hi = total * (k + 1) / nt;
-        uint64_t at = 0;
-        for (const copy_job &j : jobs) {
-            const uint64_t a = std::max(lo, at), b = std::min(hi, at + j.bytes);
-            if (a < b) {
-                char *d = static_cast<char *>(j.dst) + (a - at);
-                if (j.src) memcpy(d, static_cast<const char *>(j.src) + (a - at), b - a);
-                else memset(d, 0, b - a);
-            }
-            at += j.bytes;
-            if (at >= hi) break;
+    uint64_t at = 0;
+    for (const copy_job &j : jobs) {
+        const uint64_t a = std::max(lo, at), b = std::min(hi, at + j.bytes);
+        if (a < b) {
+            char *d = static_cast<char *>(j.dst) + (a - at);
+            if (j.src) memcpy(d, static_cast<const char *>(j.src) + (a - at), b - a);
+            else memset(d, 0, b - a);
         }
-    };
-    if (nt == 1) {
-        part(0);
-        return;
+        at += j.bytes;
+        if (at >= hi) break;
     }
-    // parts whose thread could not be started are copied here
-    std::vector<std::thread> th;
-    std::vector<unsigned> mine{0};
-    for (unsigned k = 1; k < nt; k++) {
-        try {
-            th.emplace_back(part, k);
-        } catch (const std::system_error &) {
-            mine.push_back(k);
-        }
-    }
-    for (unsigned k : mine) part(k);
-    for (std::thread &t : th) t.join();
 }
+
+// Host threads that share a wave's copies into and out of pinned staging with
+// the worker.  One thread's memcpy moves a fraction of what host memory and
+// the PCIe link take (about 11 GB/s here), and waves under load hold tens of
+// thousands of keys, so any copy of more than kCopyPart bytes is cut into
+// equal parts of at least that size, taken by the worker and up to 8 pool
+// threads (half the host's hardware threads at most).  The threads live as
+// long as the server; a copy costs a wake-up, not a thread start.
+struct copy_pool {
+    static constexpr uint64_t kCopyPart = 128 << 10;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable go, finished;
+    const std::vector<copy_job> *jobs = nullptr;
+    uint64_t total = 0, gen = 0;
+    unsigned nparts = 0, next = 0, done = 0;
+    bool stop = false;
+
+    void start()
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = std::min(8u, hw / 2);
+        for (unsigned k = 0; k < n; k++) {
+            try {
+                threads.emplace_back([this] { serve(); });
+            } catch (const std::system_error &) {
+                break;  // fewer helpers: the worker copies more itself
+            }
+        }
+    }
+    void shutdown()
+    {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            stop = true;
+        }
+        go.notify_all();
+        for (std::thread &t : threads) t.join();
+        threads.clear();
+    }
+    ~copy_pool() { shutdown(); }
+    // take parts of the current copy until none is left (lock held on entry and exit)
+    void take_parts(std::unique_lock<std::mutex> &lk)
+    {
+        while (next < nparts) {
+            const unsigned k = next++;
+            const uint64_t lo = total * k / nparts, hi = total * (k + 1) / nparts;
+            lk.unlock();
+            copy_range(*jobs, lo, hi);
+            lk.lock();
+            if (++done == nparts) finished.notify_all();
+        }
+    }
+    void serve()
+    {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            go.wait(lk, [&] { return stop || gen != seen; });
+            if (stop) return;
+            seen = gen;
+            take_parts(lk);
+        }
+    }
+    // Run the copies of one wave; returns when every byte is copied.
+    void run(const std::vector<copy_job> &js)
+    {
+        uint64_t t = 0;
+        for (const copy_job &j : js) t += j.bytes;
+        const uint64_t want = t / kCopyPart;
+        const unsigned parts = (unsigned)std::min<uint64_t>(want, threads.size() + 1);
+        if (parts <= 1) {
+            copy_range(js, 0, t);
+            return;
+        }
+        std::unique_lock<std::mutex> lk(mu);
+        jobs = &js;
+        total = t;
+        nparts = parts;
+        next = 0;
+        done = 0;
+        gen++;
+        go.notify_all();
+        take_parts(lk);
+        finished.wait(lk, [&] { return done == nparts; });
+        jobs = nullptr;
+    }
+};
 
 // What a wave's copies and launches need from the server's tables, read
 // while the lock is held: client threads may add tables meanwhile, which
@@ -285,7 +350,7 @@ struct wave_plan {
 // Copy a finished wave's results out of the pinned staging buffers into the
 // clients' buffers (without the lock: the requests belong to the worker until
 // they are published).
-void complete_stage(pg_server::stage &st, const wave_plan &pl)
+void complete_stage(copy_pool &pool, pg_server::stage &st, const wave_plan &pl)
 {
     std::vector<copy_job> jobs;
     for (size_t i = 0; i < pl.reqs.size(); i++) {
@@ -299,7 +364,7 @@ void complete_stage(pg_server::stage &st, const wave_plan &pl)
         if (r->flags) jobs.push_back({r->flags, st.h_flags + o, r->n});
         if (r->op == PG_OP_QUERY && r->vals_out && vb) jobs.push_back({r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb});
     }
-    copy_all(jobs);
+    pool.run(jobs);
     const double t = now_s();
     for (size_t i = 0; i < pl.reqs.size(); i++) {
         pl.reqs[i]->count = st.h_counts[i];
@@ -310,6 +375,8 @@ void complete_stage(pg_server::stage &st, const wave_plan &pl)
 void worker_loop(pg_server *s)
 {
     cudaSetDevice(s->device);
+    copy_pool pool;
+    pool.start();
     struct slot_state {
         wave_plan plan;
         bool busy = false;
@@ -324,8 +391,11 @@ void worker_loop(pg_server *s)
             if (!slots[w].busy) continue;
             if (cudaEventQuery(s->stages[w].done) == cudaSuccess) {
                 lk.unlock();
-                complete_stage(s->stages[w], slots[w].plan);
+                const double c0 = now_s();
+                complete_stage(pool, s->stages[w], slots[w].plan);
+                const double c1 = now_s();
                 lk.lock();
+                s->t_copy_out += c1 - c0;
                 for (request *r : slots[w].plan.reqs) {
                     if (r->slab >= 0) s->slabs[r->table].inflight--;
                     else s->tables[r->table].inflight--;
@@ -350,6 +420,7 @@ void worker_loop(pg_server *s)
                 break;
             }
         if (w >= 0 && !s->pending.empty()) {
+            const double p0 = now_s();
             bool any_dirty = false;
             for (auto &k : s->classes) any_dirty |= k.dirty;
             if (any_dirty) {
@@ -400,6 +471,7 @@ void worker_loop(pg_server *s)
                 pl.runs.back().count++;
             }
             pl.nkeys = ko;
+            const double p1 = now_s();
             lk.unlock();
             // stage keys and values in pinned memory
             std::vector<copy_job> jobs;
@@ -423,7 +495,8 @@ void worker_loop(pg_server *s)
                 if (r->op == PG_OP_QUERY && vb) any_q[width_index(vb)] = true;
                 st.h_ops[i] = pg_op_desc{pl.slot[i], r->op, o, r->n};
             }
-            copy_all(jobs);
+            pool.run(jobs);
+            const double p2 = now_s();
             // one copy in (upload stream), one run per class (its own stream,
             // after the upload), one copy out (download stream, after every run)
             for (size_t ci = 0; ci < pl.runs.size(); ci++) st.h_nops[ci] = pl.runs[ci].count;
@@ -470,23 +543,31 @@ void worker_loop(pg_server *s)
                     cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->down);
             cudaMemcpyAsync(st.h_counts, st.d_counts, nr * 8, cudaMemcpyDeviceToHost, s->down);
             cudaEventRecord(st.done, s->down);
+            const double p3 = now_s();
             lk.lock();
+            s->t_plan += p1 - p0;
+            s->t_copy_in += p2 - p1;
+            s->t_issue += p3 - p2;
             if (launch_error != PG_OK) s->error = launch_error;
             slots[w].busy = true;
             s->waves_run++;
             s->keys_run += ko;
+            s->requests_run += nr;
             next_slot = (w + 1) % kMaxWaves;
             continue;
         }
         // 3. nothing to launch: wait for work or for a wave to finish
         bool any_busy = false;
         for (auto &sl : slots) any_busy |= sl.busy;
+        const double w0 = now_s();
         if (any_busy) {
             lk.unlock();
             std::this_thread::sleep_for(std::chrono::microseconds(20));
             lk.lock();
+            s->t_wait_busy += now_s() - w0;
         } else {
             s->cv.wait_for(lk, std::chrono::milliseconds(2));
+            s->t_wait_idle += now_s() - w0;
         }
     }
 }
@@ -786,6 +867,22 @@ pg_status pg_server_poll(pg_server *s, uint64_t request_id, int wait, uint64_t *
         if (!wait) return PG_ERR_TIMEOUT;  // not finished yet
         s->cv.wait_for(lk, std::chrono::milliseconds(1));
     }
+}
+
+pg_status pg_server_timing(pg_server *s, pg_server_timing_t *out)
+{
+    if (!s || !out) return PG_ERR_INVALID;
+    std::lock_guard<std::mutex> g(s->mu);
+    out->waves = s->waves_run;
+    out->requests = s->requests_run;
+    out->keys = s->keys_run;
+    out->plan_s = s->t_plan;
+    out->copy_in_s = s->t_copy_in;
+    out->issue_s = s->t_issue;
+    out->copy_out_s = s->t_copy_out;
+    out->wait_busy_s = s->t_wait_busy;
+    out->wait_idle_s = s->t_wait_idle;
+    return PG_OK;
 }
 
 pg_status pg_server_stats(pg_server *s, uint64_t *waves, uint64_t *keys)
