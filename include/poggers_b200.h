@@ -208,6 +208,14 @@ pg_status pg_scatter_by_perm(const void *d_src, const uint32_t *d_perm, uint64_t
  * placed by the same rule.  The scratch is the table's: two region-ordered
  * inserts into one table must be ordered on one stream. */
 pg_status pg_table_set_partitioned_insert(pg_table *t, int enable);
+/* Whether a fingerprinted table's fingerprint array is treated as L2-resident
+ * (default: when it is at most 80 MB).  Resident, its loads are marked
+ * evict-last and a query reads two buckets' fingerprints per step; not
+ * resident, loads are plain and a query reads one bucket per step.  Results
+ * are the same either way.  Batches take the setting when they are created.
+ * PG_ERR_INVALID for a table without fingerprints.  No counterpart in the
+ * reference. */
+pg_status pg_table_set_fingerprint_residency(pg_table *t, int resident);
 /* Grow the region sort's scratch for insert batches of up to max_batch_keys
  * keys (ordered on `stream`); PG_ERR_NOMEM if it cannot be allocated.  No
  * counterpart in the reference. */

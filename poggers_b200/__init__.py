@@ -97,7 +97,7 @@ EXPORTED = (
     "pg_slab_bulk_free", "pg_slab_count_free", "pg_slab_report", "pg_slab_desc", "pg_slab_set_create", "pg_slab_set_destroy",
     "pg_slab_set_class", "pg_slab_set_bulk_malloc", "pg_slab_set_bulk_free",
     "pg_batch_create", "pg_batch_destroy", "pg_batch_set_launch", "pg_batch_run", "pg_batch_run_static",
-    "pg_batch_clear", "pg_table_reserve_insert_scratch",
+    "pg_batch_clear", "pg_table_reserve_insert_scratch", "pg_table_set_fingerprint_residency",
     "pg_pslab_create", "pg_pslab_destroy", "pg_pslab_desc", "pg_pslab_report", "pg_pslab_bulk_malloc",
     "pg_pslab_serial_malloc", "pg_pslab_bulk_free",
     "pg_server_create", "pg_server_destroy", "pg_server_add_table", "pg_server_drop_table", "pg_server_table",
@@ -214,6 +214,8 @@ def lib() -> C.CDLL:
     L.pg_pslab_bulk_free.argtypes = [V, P, U64, P, C.c_int, P]
     L.pg_table_reserve_insert_scratch.restype = C.c_int
     L.pg_table_reserve_insert_scratch.argtypes = [V, U64, P]
+    L.pg_table_set_fingerprint_residency.restype = C.c_int
+    L.pg_table_set_fingerprint_residency.argtypes = [V, C.c_int]
     L.pg_batch_clear.restype = C.c_int
     L.pg_batch_clear.argtypes = [V, P]
     L.pg_batch_run_static.restype = C.c_int
@@ -378,6 +380,11 @@ class Table:
         """Grow the region sort's scratch ahead of time (pg_table_reserve_insert_scratch)."""
         _check(lib().pg_table_reserve_insert_scratch(self._h, max_batch_keys, _stream(stream)),
                "pg_table_reserve_insert_scratch")
+
+    def set_fingerprint_residency(self, resident: bool) -> None:
+        """Treat the fingerprint array as L2-resident or not (pg_table_set_fingerprint_residency)."""
+        _check(lib().pg_table_set_fingerprint_residency(self._h, int(bool(resident))),
+               "pg_table_set_fingerprint_residency")
 
     def set_partitioned_insert(self, enable: bool) -> None:
         """Region-ordered inserts for large batches (on by default)."""

@@ -399,6 +399,13 @@ pg_status pg_table_set_partitioned_insert(pg_table *t, int enable)
     return PG_OK;
 }
 
+pg_status pg_table_set_fingerprint_residency(pg_table *t, int resident)
+{
+    if (!t || !t->fp) return PG_ERR_INVALID;
+    t->desc.lv[0].fp_resident = resident != 0;
+    return PG_OK;
+}
+
 pg_status pg_table_reserve_insert_scratch(pg_table *t, uint64_t max_batch_keys, pg_stream_t stream)
 {
     if (!t || !pg_on_device(t->device)) return PG_ERR_INVALID;

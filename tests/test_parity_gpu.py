@@ -414,6 +414,33 @@ def test_fingerprints_with_backing_level_matches_oracle(pg, oracle):
     assert (f[:n] == ok).all()
 
 
+@pytest.mark.parametrize("resident", [True, False])
+@pytest.mark.parametrize("backing", [False, True])
+def test_fingerprint_query_both_step_widths_match_oracle(pg, oracle, resident, backing):
+    """The lane-refill query reads two buckets' fingerprints per step while the
+    fingerprint array is L2-resident and one otherwise (tables past 80 MB of
+    fingerprints); forcing the setting on a small table checks both widths
+    against the oracle, with and without a backing level, on present and
+    absent keys."""
+    levels = [(1 << 20, 8, 20, 0, 0)] + ([(1 << 14, 8, 20, 0, 0)] if backing else [])
+    cfg = pg.TableConfig(pg.FMT_KV64, 4, [pg.Level(*lv) for lv in levels])
+    cfg.fingerprints = True
+    t = pg.Table(cfg, 21)
+    t.set_fingerprint_residency(resident)
+    d = Driver(t)
+    o = oracle.OracleTable(0, 4, levels, 21)
+    n = int(0.95 * (1 << 20))
+    keys = wl.keys_without_sentinels(51, n)
+    vals = wl.values_for(keys, 8, 52)
+    q = np.concatenate([keys, wl.keys_without_sentinels(53, 1 << 18)])
+    ok, oko = d.insert(keys, vals), o.insert_many(keys, vals)
+    both = np.concatenate([ok & oko, np.ones(1 << 18, dtype=bool)])
+    f, v = d.query(q)
+    fo, vo = o.query_many(q)
+    assert (f[both] == fo[both]).all() and (v[both] == vo[both]).all()
+    assert (f[:n] == ok).all() and (v[:n][ok] == vals[ok]).all()
+
+
 @pytest.mark.parametrize("layout", LAYOUTS)
 def test_slot_cas_succeeds_once_under_contention(pg, layout):
     """key_val_pair::atomic_swap succeeds once per empty slot
