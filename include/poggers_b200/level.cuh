@@ -943,11 +943,19 @@ struct level_ops_fp {
     __device__ static bool insert_s(const level_desc &L, const group<1> &, uint64_t key, V val)
     {
         static_assert(SCHEME == SCHEME_BUCKET, "fingerprints index bucket_insert levels");
+        return insert_probes(L, key, val, 0, L.max_probes);
+    }
+    // The insert over probes [i0, i1) of the key's sequence: true when placed.
+    // A bucket found full stays full (fill only grows during inserts), so a
+    // caller may try probe 0 first and the rest later with the same result.
+    __device__ __forceinline__ static bool insert_probes(const level_desc &L, uint64_t key, V val, uint32_t i0,
+                                                         uint32_t i1)
+    {
         probe_seq ps;
         ps.begin(L.probe, key, key, L.seed, L.seed2);
         const uint32_t f = fp_of(key, ps.h1);
         const uint64_t keep = fp_policy(L);
-        for (uint32_t i = 0; i < L.max_probes; ++i) {
+        for (uint32_t i = i0; i < i1 && i < L.max_probes; ++i) {
             const uint64_t raw = ps.at(i);
             if (raw == kProbeEnd) break;
             const uint64_t b = L.nbmod.mod(raw);

@@ -141,6 +141,57 @@ __global__ void __launch_bounds__(256, TWO ? PG_FP_QUERY_MIN_BLOCKS : 8) k_query
     add_count(a.count, hits);
 }
 
+// Region-ordered insert (the sorted runs of partition.cu), one thread per
+// entry with blocks in batch order, so the resident blocks sweep the table
+// region by region.  Each key tries its first probe; a key whose first bucket
+// is full (about one in eight at 0.9 load) joins the block's queue, and once
+// the block's first attempts are done its threads take the queued keys
+// together, from their second probe on (then the backing level).  Without the
+// queue a warp runs every later probe of its slowest lane with most lanes idle.
+#ifndef PG_FP_INSERT_QUEUE
+#define PG_FP_INSERT_QUEUE 1
+#endif
+template <int B, bool BK>
+__global__ void __launch_bounds__(256, PG_FP_MIN_BLOCKS) k_insert_fp_runs(table_desc t, bulk_args a)
+{
+    using P = level_ops_fp<B>;
+    using BKO = backing_ops<FMT_KV64, 1>;
+    __shared__ uint32_t queue[256];
+    __shared__ uint32_t qn;
+    if (threadIdx.x == 0) qn = 0;
+    __syncthreads();
+    const level_desc &L = t.lv[0];
+    const unsigned long long *vin = static_cast<const unsigned long long *>(a.vals_in);
+    const uint64_t base = (uint64_t)blockIdx.x * blockDim.x;
+    const uint64_t i = base + threadIdx.x;
+    bool live = i < a.n;
+    if (live) {
+        // past the keys of this region's run: nothing there
+        const uint64_t r = __umul64hi(a.region_div, i);
+        live = i - r * a.region_cap < a.region_cursor[r] - r * a.region_cap;
+    }
+    if (live) {
+        const uint64_t key = __ldg(a.keys + i);
+        const unsigned long long v = vin ? __ldg(vin + i) : 0ULL;
+        if (!P::insert_probes(L, key, v, 0, 1)) queue[atomicAdd(&qn, 1u)] = threadIdx.x;
+    }
+    __syncthreads();
+    const uint32_t nq = qn;
+    uint32_t fails = 0;
+    for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x) {
+        const uint64_t j = base + queue[q];
+        const uint64_t key = __ldg(a.keys + j);
+        const unsigned long long v = vin ? __ldg(vin + j) : 0ULL;
+        bool r = P::insert_probes(L, key, v, 1, L.max_probes);
+        if (!r && BK && t.nlevels > 1) r = BKO::insert(t.lv[1], group<1>::make(), key, v);
+        if (!r) {
+            if (a.flags) a.flags[a.perm[j]] = 0;
+            fails++;
+        }
+    }
+    add_count(a.count, fails);
+}
+
 // resident 256-thread blocks of a kernel on the current device (0 if unknown);
 // looked up once per (device, kernel), under a lock so host threads may launch
 // concurrently
@@ -196,6 +247,13 @@ template <int B>
 cudaError_t launch_fp_b(int op, const table_desc &t, const bulk_args &a, dim3 grid, dim3 block, cudaStream_t s)
 {
     const bool bk = t.nlevels > 1;
+    // the sorted runs of a region-ordered insert (one thread per entry; see k_insert_fp_runs)
+    if (PG_FP_INSERT_QUEUE && op == OP_INSERT && a.region_cap && !a.only && block.x == 256 && a.perm) {
+        const uint64_t blocks = (a.n + 255) / 256;
+        if (bk) k_insert_fp_runs<B, true><<<(unsigned)blocks, 256, 0, s>>>(t, a);
+        else k_insert_fp_runs<B, false><<<(unsigned)blocks, 256, 0, s>>>(t, a);
+        return cudaGetLastError();
+    }
     // the refill query needs whole warps; the serial shape (one lane) keeps the plain kernel
     if (op == OP_QUERY && block.x == 256 && grid.x > 1)
         return bk ? launch_query_refill<B, true>(t, a, grid, s) : launch_query_refill<B, false>(t, a, grid, s);
