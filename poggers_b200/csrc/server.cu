@@ -109,16 +109,10 @@ struct pg_server {
     std::deque<request *> pending;
     std::map<uint64_t, request *> done;
     std::set<uint64_t> outstanding;  // submitted and not yet collected by pg_server_poll
-    // staging (per wave slot): pinned host and device buffers
+    // staging (per wave slot): one pinned host buffer and one device buffer,
+    // laid out per wave (wave_layout)
     struct stage {
-        uint64_t *h_keys, *d_keys;
-        // values by width (8, 2 and 1 bytes: uint64 tables, 16- and 8-bit
-        // filters), each indexed like the keys; see width_index
-        unsigned char *h_vin[3], *d_vin[3], *h_vout[3], *d_vout[3];
-        uint8_t *h_flags, *d_flags;
-        pg_op_desc *h_ops, *d_ops;
-        uint32_t *h_nops, *d_nops;
-        uint64_t *h_counts, *d_counts;
+        unsigned char *h, *d;
         cudaEvent_t uploaded;  // the wave's inputs are on the device
         cudaEvent_t ran;       // recorded after each class's run, waited on by the download stream
         cudaEvent_t done;
@@ -147,6 +141,49 @@ bool conflicts(uint32_t a, uint32_t b) { return a != b; }
 // staging buffer of a value width: 8 -> 0, 2 -> 1, 1 -> 2
 int width_index(uint32_t vb) { return vb == 8 ? 0 : vb == 2 ? 1 : 2; }
 constexpr uint32_t kWidths[3] = {8, 2, 1};
+
+// Where one wave's inputs and outputs sit in its stage's buffers, at the same
+// offsets on the host and on the device: the keys (a malloc's sizes and a
+// free's pointers too), the values in by width, the requests, each class run's
+// request count and the per-request counts are uploaded together, [0, up_end);
+// the counts, the flags and the values out by width come back together,
+// [counts, end).  Values are indexed like the keys; a width no request of the
+// wave uses takes no room.
+struct wave_layout {
+    uint64_t keys, vin[3], ops, nops, counts, up_end, flags, vout[3], end;
+    bool has_in[3], has_out[3];
+};
+
+uint64_t align16(uint64_t x) { return (x + 15) & ~15ull; }
+
+wave_layout lay_out(uint64_t nkeys, uint64_t nreqs, uint64_t nruns, const bool in[3], const bool out[3])
+{
+    wave_layout L{};
+    uint64_t at = 0;
+    L.keys = at;
+    at = align16(at + nkeys * 8);
+    for (int x = 0; x < 3; x++) {
+        L.has_in[x] = in[x];
+        L.vin[x] = at;
+        if (in[x]) at = align16(at + nkeys * kWidths[x]);
+    }
+    L.ops = at;
+    at = align16(at + nreqs * sizeof(pg_op_desc));
+    L.nops = at;
+    at = align16(at + nruns * 4);
+    L.counts = at;
+    at = align16(at + nreqs * 8);
+    L.up_end = at;
+    L.flags = at;
+    at = align16(at + nkeys);
+    for (int x = 0; x < 3; x++) {
+        L.has_out[x] = out[x];
+        L.vout[x] = at;
+        if (out[x]) at = align16(at + nkeys * kWidths[x]);
+    }
+    L.end = at;
+    return L;
+}
 
 // wait for every wave the server has issued (uploads, every class's runs, downloads)
 void sync_all(pg_server *s)
@@ -345,6 +382,7 @@ struct wave_plan {
     };
     std::vector<slab_run> slab_runs;  // one bulk malloc / free per slab request
     uint64_t nkeys = 0;
+    wave_layout lay{};
 };
 
 // Copy a finished wave's results out of the pinned staging buffers into the
@@ -358,16 +396,18 @@ void complete_stage(copy_pool &pool, pg_server::stage &st, const wave_plan &pl)
         const uint64_t o = pl.key_off[i];
         const uint32_t vb = pl.vb[i];
         if (r->slab >= 0) {
-            if (r->op == PG_OP_MALLOC && r->vals_out) jobs.push_back({r->vals_out, st.h_vout[0] + o * 8, r->n * 8});
+            if (r->op == PG_OP_MALLOC && r->vals_out) jobs.push_back({r->vals_out, st.h + pl.lay.vout[0] + o * 8, r->n * 8});
             continue;
         }
-        if (r->flags) jobs.push_back({r->flags, st.h_flags + o, r->n});
-        if (r->op == PG_OP_QUERY && r->vals_out && vb) jobs.push_back({r->vals_out, st.h_vout[width_index(vb)] + o * vb, r->n * vb});
+        if (r->flags) jobs.push_back({r->flags, st.h + pl.lay.flags + o, r->n});
+        if (r->op == PG_OP_QUERY && r->vals_out && vb)
+            jobs.push_back({r->vals_out, st.h + pl.lay.vout[width_index(vb)] + o * vb, r->n * vb});
     }
     pool.run(jobs);
     const double t = now_s();
+    const uint64_t *counts = reinterpret_cast<const uint64_t *>(st.h + pl.lay.counts);
     for (size_t i = 0; i < pl.reqs.size(); i++) {
-        pl.reqs[i]->count = st.h_counts[i];
+        pl.reqs[i]->count = counts[i];
         pl.reqs[i]->t_done = t;
     }
 }
@@ -473,48 +513,62 @@ void worker_loop(pg_server *s)
             pl.nkeys = ko;
             const double p1 = now_s();
             lk.unlock();
+            // which value widths the wave moves, then its layout
+            bool any_in[3] = {false, false, false}, any_q[3] = {false, false, false};
+            for (size_t i = 0; i < nr; i++) {
+                const request *r = pl.reqs[i];
+                const uint32_t vb = pl.vb[i];
+                if (r->slab >= 0) {
+                    if (r->op == PG_OP_MALLOC) any_q[0] = true;  // the objects' addresses come back as 8-byte values
+                } else if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
+                    any_in[width_index(vb)] = true;
+                } else if (r->op == PG_OP_QUERY && vb) {
+                    any_q[width_index(vb)] = true;
+                }
+            }
+            pl.lay = lay_out(ko, nr, pl.runs.size(), any_in, any_q);
+            const wave_layout &lay = pl.lay;
             // stage keys and values in pinned memory
             std::vector<copy_job> jobs;
-            bool any_in[3] = {false, false, false}, any_q[3] = {false, false, false};
+            pg_op_desc *h_ops = reinterpret_cast<pg_op_desc *>(st.h + lay.ops);
             for (size_t i = 0; i < nr; i++) {
                 request *r = pl.reqs[i];
                 const uint64_t o = pl.key_off[i];
                 const uint32_t vb = pl.vb[i];
                 if (r->slab >= 0) {
                     // malloc: n sizes of 4 bytes; free: n pointers; both fit the keys' 8 bytes each
-                    jobs.push_back({st.h_keys + o, r->keys, r->n * (r->op == PG_OP_MALLOC ? 4 : 8)});
-                    if (r->op == PG_OP_MALLOC) any_q[0] = true;
-                    st.h_ops[i] = pg_op_desc{0, r->op, o, r->n};
+                    jobs.push_back({st.h + lay.keys + o * 8, r->keys, r->n * (r->op == PG_OP_MALLOC ? 4 : 8)});
+                    h_ops[i] = pg_op_desc{0, r->op, o, r->n};
                     continue;
                 }
-                jobs.push_back({st.h_keys + o, r->keys, r->n * 8});
-                if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb) {
-                    jobs.push_back({st.h_vin[width_index(vb)] + o * vb, r->vals, r->n * vb});
-                    any_in[width_index(vb)] = true;
-                }
-                if (r->op == PG_OP_QUERY && vb) any_q[width_index(vb)] = true;
-                st.h_ops[i] = pg_op_desc{pl.slot[i], r->op, o, r->n};
+                jobs.push_back({st.h + lay.keys + o * 8, r->keys, r->n * 8});
+                if ((r->op == PG_OP_INSERT || r->op == PG_OP_INSERT_WITH_DELETE) && vb)
+                    jobs.push_back({st.h + lay.vin[width_index(vb)] + o * vb, r->vals, r->n * vb});
+                h_ops[i] = pg_op_desc{pl.slot[i], r->op, o, r->n};
             }
             pool.run(jobs);
             const double p2 = now_s();
+            uint32_t *h_nops = reinterpret_cast<uint32_t *>(st.h + lay.nops);
+            for (size_t ci = 0; ci < pl.runs.size(); ci++) h_nops[ci] = pl.runs[ci].count;
+            memset(st.h + lay.counts, 0, nr * 8);
             // one copy in (upload stream), one run per class (its own stream,
             // after the upload), one copy out (download stream, after every run)
-            for (size_t ci = 0; ci < pl.runs.size(); ci++) st.h_nops[ci] = pl.runs[ci].count;
-            cudaMemcpyAsync(st.d_keys, st.h_keys, ko * 8, cudaMemcpyHostToDevice, s->stream);
-            for (int x = 0; x < 3; x++)
-                if (any_in[x])
-                    cudaMemcpyAsync(st.d_vin[x], st.h_vin[x], ko * kWidths[x], cudaMemcpyHostToDevice, s->stream);
-            cudaMemcpyAsync(st.d_ops, st.h_ops, nr * sizeof(pg_op_desc), cudaMemcpyHostToDevice, s->stream);
-            cudaMemcpyAsync(st.d_nops, st.h_nops, pl.runs.size() * 4, cudaMemcpyHostToDevice, s->stream);
-            cudaMemsetAsync(st.d_counts, 0, nr * 8, s->stream);
+            cudaMemcpyAsync(st.d, st.h, lay.up_end, cudaMemcpyHostToDevice, s->stream);
             cudaEventRecord(st.uploaded, s->stream);
+            unsigned char *d = st.d;
+            uint64_t *d_keys = reinterpret_cast<uint64_t *>(d + lay.keys);
+            pg_op_desc *d_ops = reinterpret_cast<pg_op_desc *>(d + lay.ops);
+            uint32_t *d_nops = reinterpret_cast<uint32_t *>(d + lay.nops);
+            uint64_t *d_counts = reinterpret_cast<uint64_t *>(d + lay.counts);
+            uint8_t *d_flags = d + lay.flags;
             pg_status launch_error = PG_OK;
             for (size_t ci = 0; ci < pl.runs.size(); ci++) {
                 const wave_plan::run &rn = pl.runs[ci];
                 cudaStreamWaitEvent(rn.stream, st.uploaded, 0);
                 const int x = width_index(rn.vb);
-                pg_status rs = pg_batch_run(rn.batch, st.d_ops + rn.first, st.d_nops + ci, st.d_keys, st.d_vin[x],
-                                            st.d_vout[x], st.d_flags, st.d_counts + rn.first,
+                pg_status rs = pg_batch_run(rn.batch, d_ops + rn.first, d_nops + ci, d_keys,
+                                            lay.has_in[x] ? d + lay.vin[x] : nullptr,
+                                            lay.has_out[x] ? d + lay.vout[x] : nullptr, d_flags, d_counts + rn.first,
                                             reinterpret_cast<pg_stream_t>(rn.stream));
                 if (rs != PG_OK) launch_error = rs;
                 // the download waits for this run (a wait takes the event's latest record)
@@ -527,21 +581,17 @@ void worker_loop(pg_server *s)
                 cudaStreamWaitEvent(sr.stream, st.uploaded, 0);
                 pg_status rs;
                 if (r->op == PG_OP_MALLOC)
-                    rs = pg_slab_set_bulk_malloc(sr.set, reinterpret_cast<const uint32_t *>(st.d_keys + o), r->n,
-                                                 reinterpret_cast<void **>(st.d_vout[0] + o * 8), st.d_counts + sr.req,
+                    rs = pg_slab_set_bulk_malloc(sr.set, reinterpret_cast<const uint32_t *>(d_keys + o), r->n,
+                                                 reinterpret_cast<void **>(d + lay.vout[0] + o * 8), d_counts + sr.req,
                                                  reinterpret_cast<pg_stream_t>(sr.stream));
                 else
-                    rs = pg_slab_set_bulk_free(sr.set, reinterpret_cast<void *const *>(st.d_keys + o), r->n,
-                                               st.d_counts + sr.req, reinterpret_cast<pg_stream_t>(sr.stream));
+                    rs = pg_slab_set_bulk_free(sr.set, reinterpret_cast<void *const *>(d_keys + o), r->n,
+                                               d_counts + sr.req, reinterpret_cast<pg_stream_t>(sr.stream));
                 if (rs != PG_OK) launch_error = rs;
                 cudaEventRecord(st.ran, sr.stream);
                 cudaStreamWaitEvent(s->down, st.ran, 0);
             }
-            cudaMemcpyAsync(st.h_flags, st.d_flags, ko, cudaMemcpyDeviceToHost, s->down);
-            for (int x = 0; x < 3; x++)
-                if (any_q[x])
-                    cudaMemcpyAsync(st.h_vout[x], st.d_vout[x], ko * kWidths[x], cudaMemcpyDeviceToHost, s->down);
-            cudaMemcpyAsync(st.h_counts, st.d_counts, nr * 8, cudaMemcpyDeviceToHost, s->down);
+            cudaMemcpyAsync(st.h + lay.counts, d + lay.counts, lay.end - lay.counts, cudaMemcpyDeviceToHost, s->down);
             cudaEventRecord(st.done, s->down);
             const double p3 = now_s();
             lk.lock();
@@ -586,25 +636,14 @@ pg_status pg_server_create(const pg_server_config *cfg, pg_server **out)
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking);
     const uint64_t K = cfg->max_wave_keys, R = cfg->max_wave_requests;
+    // the largest wave: every width in and out (one class run per request at most)
+    const bool all[3] = {true, true, true};
+    const uint64_t stage_bytes = lay_out(K, R, R, all, all).end;
     for (int w = 0; w < kMaxWaves && e == cudaSuccess; w++) {
         auto &st = s->stages[w];
         memset(&st, 0, sizeof(st));
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_keys, K * 8);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_keys, K * 8);
-        for (int x = 0; x < 3; x++) {
-            if (e == cudaSuccess) e = cudaMallocHost(&st.h_vin[x], K * kWidths[x]);
-            if (e == cudaSuccess) e = cudaMalloc(&st.d_vin[x], K * kWidths[x]);
-            if (e == cudaSuccess) e = cudaMallocHost(&st.h_vout[x], K * kWidths[x]);
-            if (e == cudaSuccess) e = cudaMalloc(&st.d_vout[x], K * kWidths[x]);
-        }
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_flags, K);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_flags, K);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_ops, R * sizeof(pg_op_desc));
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_ops, R * sizeof(pg_op_desc));
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_nops, R * 4);  // one run per class, at most one per request
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_nops, R * 4);
-        if (e == cudaSuccess) e = cudaMallocHost(&st.h_counts, R * 8);
-        if (e == cudaSuccess) e = cudaMalloc(&st.d_counts, R * 8);
+        if (e == cudaSuccess) e = cudaMallocHost(&st.h, stage_bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&st.d, stage_bytes);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.uploaded, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.ran, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming);
@@ -639,22 +678,8 @@ pg_status pg_server_destroy(pg_server *s)
         if (e.stream) cudaStreamDestroy(e.stream);
     }
     for (auto &st : s->stages) {
-        cudaFreeHost(st.h_keys);
-        cudaFree(st.d_keys);
-        for (int x = 0; x < 3; x++) {
-            cudaFreeHost(st.h_vin[x]);
-            cudaFree(st.d_vin[x]);
-            cudaFreeHost(st.h_vout[x]);
-            cudaFree(st.d_vout[x]);
-        }
-        cudaFreeHost(st.h_flags);
-        cudaFree(st.d_flags);
-        cudaFreeHost(st.h_ops);
-        cudaFree(st.d_ops);
-        cudaFreeHost(st.h_nops);
-        cudaFree(st.d_nops);
-        cudaFreeHost(st.h_counts);
-        cudaFree(st.d_counts);
+        cudaFreeHost(st.h);
+        cudaFree(st.d);
         if (st.uploaded) cudaEventDestroy(st.uploaded);
         if (st.ran) cudaEventDestroy(st.ran);
         if (st.done) cudaEventDestroy(st.done);
