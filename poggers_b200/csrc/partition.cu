@@ -30,6 +30,7 @@ constexpr uint32_t kPartThreads = 256;
 constexpr uint32_t kPartPerThread = 4;
 constexpr uint32_t kPartTile = kPartThreads * kPartPerThread;  // keys per scatter tile
 constexpr uint32_t kPartMaxRegions = 1024;
+static_assert(kPartTile <= 65536 && kPartMaxRegions <= 65536, "a staged entry's tag packs region and index in 16 bits each");
 #ifndef PG_PART_REGION_MB
 #define PG_PART_REGION_MB 32
 #endif
@@ -114,12 +115,21 @@ __global__ void k_part_bases(unsigned long long *cursors, uint32_t R, uint64_t c
 // the cap entries from r * cap; a key reserved past them is not written and
 // its bit (by its index in the batch) is set in ovf instead.
 // The per-region arrays take part_scatter_smem(R) bytes of dynamic shared
-// memory (22.5 KB per block in all at 32 regions instead of 38.9 KB sized for
-// the most regions; more resident blocks, forced by register limits of 40 or
-// 32, measured 2 % slower).  Tiles of 4 keys per thread: 2 measured 9 %
-// slower for the whole insert call, 8 the same (ncu: issue-bound with barrier
-// and shared-memory stalls at 45 % of DRAM peak, not bound by DRAM).
+// memory beside the 20 KB of staged entries (more resident blocks, forced by
+// register limits of 40 or 32, measured 2 % slower).  Tiles of 4 keys per
+// thread: 2 measured 9 % slower for the whole insert call, 8 the same (ncu:
+// issue-bound with barrier and shared-memory stalls at 45 % of DRAM peak, not
+// bound by DRAM).  Staging key and value as one 16-byte entry with region and
+// index packed in one word, and each region's output offset computed once per
+// tile, took the kernel from 534 to 500 us at 2^26 slots.
 inline size_t part_scatter_smem(uint32_t R) { return (size_t)R * (sizeof(unsigned long long) + 2 * sizeof(unsigned)); }
+
+// a key and its value staged in shared memory (one 16-byte access each way)
+template <class V>
+struct __align__(16) part_entry {
+    uint64_t k;
+    V v;
+};
 
 template <class Router, class V>
 __global__ void __launch_bounds__(kPartThreads)
@@ -128,13 +138,13 @@ __global__ void __launch_bounds__(kPartThreads)
                    uint32_t *ovf)
 {
     extern __shared__ unsigned long long part_dyn[];
-    unsigned long long *gbase = part_dyn;                                 // R reservations
+    // per region: the reservation, then (once the tile is sorted) the offset
+    // from a tile position to its place in the output, gbase - lstart
+    unsigned long long *gbase = part_dyn;
     unsigned int *cnt = reinterpret_cast<unsigned int *>(gbase + R);      // R tile counts
     unsigned int *lstart = cnt + R;                                       // R tile offsets
-    __shared__ uint64_t sk[kPartTile];
-    __shared__ V sv[kPartTile];
-    __shared__ uint32_t sp[kPartTile];
-    __shared__ uint16_t sr[kPartTile];
+    __shared__ part_entry<V> skv[kPartTile];
+    __shared__ uint32_t stag[kPartTile];  // region << 16 | the entry's index in the tile
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     for (uint64_t t0 = (uint64_t)blockIdx.x * kPartTile; t0 < n; t0 += (uint64_t)gridDim.x * kPartTile) {
         const uint32_t tn = (uint32_t)((n - t0) < kPartTile ? (n - t0) : kPartTile);
@@ -185,22 +195,26 @@ __global__ void __launch_bounds__(kPartThreads)
             if (reg[j] == 0xFFFFFFFFu) continue;
             const uint32_t e = j * kPartThreads + tid;
             const uint32_t at = lstart[reg[j]] + rank[j];
-            sk[at] = k[j];
-            sv[at] = v[j];
-            sp[at] = (uint32_t)(t0 + e);
-            sr[at] = (uint16_t)reg[j];
+            skv[at] = part_entry<V>{k[j], v[j]};
+            stag[at] = (reg[j] << 16) | e;
         }
+        // the regions' offsets from tile position to output place (wraps mod 2^64 when lstart > gbase)
+        for (uint32_t r = tid; r < R; r += blockDim.x)
+            if (cnt[r]) gbase[r] -= lstart[r];
         __syncthreads();
         for (uint32_t e = tid; e < tn; e += blockDim.x) {
-            const uint32_t r = sr[e];
-            const uint64_t pos = gbase[r] + (e - lstart[r]);
+            const uint32_t tag = stag[e];
+            const uint32_t r = tag >> 16;
+            const uint32_t src = (uint32_t)t0 + (tag & 0xFFFFu);
+            const uint64_t pos = gbase[r] + e;
             if (cap && pos >= (uint64_t)(r + 1) * cap) {
-                atomicOr(ovf + (sp[e] >> 5), 1u << (sp[e] & 31u));
+                atomicOr(ovf + (src >> 5), 1u << (src & 31u));
                 continue;
             }
-            okeys[pos] = sk[e];
-            if (ovals) ovals[pos] = sv[e];
-            operm[pos] = sp[e];
+            const part_entry<V> kv = skv[e];
+            okeys[pos] = kv.k;
+            if (ovals) ovals[pos] = kv.v;
+            operm[pos] = src;
         }
         __syncthreads();
     }
