@@ -186,3 +186,58 @@ def test_reserved_scratch_means_no_allocation_in_the_insert(pg):
     assert t.host_bytes_in_use() == reserved and ok.all()
     f, v = Driver(t).query(keys)
     assert f.all() and (v == vals).all()
+
+
+def test_wide_tile_scatter_for_many_regions(pg):
+    """A table of more than 64 regions (2^28 slots, 4 GiB: 128 regions) sorts
+    with the wide-tile scatter.  The batch holds 0.8 x 2^28 distinct keys and
+    2^20 copies of one key between them, so that key's run overflows and the
+    second pass takes the rest.  The bucket rule allows a key to fail only when
+    every bucket of its probe sequence is full: checked on a dump of the level
+    for each failed key (a handful: region order fills a region's buckets
+    before the next region's keys probe into it) and for the copied key, whose
+    copies beyond its buckets' 160 slots must fail.  Every placed key is found
+    with its own value, flagged at its own batch position, and the level's
+    fill equals the keys placed."""
+    import ctypes
+    import torch
+    from oracle import pyoracle
+    ns = 1 << 28
+    nb = ns // 8
+    nu = int(0.8 * ns)
+    ndup = 1 << 20
+    cfg = pg.data_structs.hash_table_64(ns, bucket=8)
+    cfg.fingerprints = True
+    t = pg.Table(cfg, 44)
+    uniq = wl.device_splitmix64(61, nu)
+    dup_key = uniq[:1]
+    keys = torch.cat([uniq[: nu // 2], dup_key.expand(ndup), uniq[nu // 2:]])
+    vals = wl.device_splitmix64(62, nu + ndup)
+    ok = torch.zeros(nu + ndup, dtype=torch.uint8, device="cuda")
+    t.bulk_insert(keys, vals, ok)
+    is_dup = torch.zeros(nu + ndup, dtype=torch.bool, device="cuda")
+    is_dup[nu // 2: nu // 2 + ndup] = True
+    is_dup[0] = True  # uniq[0] is the duplicated key
+    okb = ok.bool()
+    failed = keys[~is_dup & ~okb].cpu().numpy().view(np.uint64)
+    assert len(failed) < 100, len(failed)
+    placed_dups = int(okb[is_dup].sum().item())
+    assert 0 < placed_dups <= 160, placed_dups
+    assert t.get_fill(0)[0] == int(okb.sum().item())
+    # a failed key's probe buckets are all full (slot key 0 = empty)
+    dump = np.empty(2 * ns, dtype=np.uint64)
+    assert pg.lib().pg_table_dump_level(t._h, 0, ctypes.c_void_p(dump.ctypes.data), dump.nbytes) == 0
+    slot_keys = dump[0::2]
+    for k in list(failed) + [int(uniq[0].item()) & ((1 << 64) - 1)]:
+        for b in {v % nb for v in pyoracle.probe_values(0, 44, 0, int(k), 20)}:
+            assert (slot_keys[8 * b: 8 * b + 8] != 0).all(), (k, b)
+    del dump, slot_keys
+    q = uniq[1:]
+    found = torch.zeros(nu - 1, dtype=torch.uint8, device="cuda")
+    qv = torch.zeros(nu - 1, dtype=torch.int64, device="cuda")
+    t.bulk_query(q, qv, found)
+    exp_ok = okb[~is_dup]
+    exp_v = vals[~is_dup]
+    assert torch.equal(found.bool(), exp_ok)
+    assert torch.equal(qv[exp_ok], exp_v[exp_ok])
+    t.free_on_device()
