@@ -559,7 +559,8 @@ pg_status pg_table_dump_level(const pg_table *t, uint32_t level, void *host_dst,
 
 pg_status pg_table_load_level(pg_table *t, uint32_t level, const void *host_src, uint64_t bytes)
 {
-    if (!t || !host_src || level >= t->cfg.nlevels) return PG_ERR_INVALID;
+    // a fingerprinted level's index is rebuilt by a kernel on the table's device
+    if (!t || !host_src || level >= t->cfg.nlevels || !pg_on_device(t->device)) return PG_ERR_INVALID;
     const level_desc &D = t->desc.lv[level];
     const uint32_t kb = key_bytes(t->cfg.format), vb = val_bytes(t->cfg.format), sb = kb + vb;
     const uint64_t nslots = D.nbmod.d * D.bucket_size;
