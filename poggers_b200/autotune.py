@@ -107,6 +107,15 @@ def best(results: list[Result]) -> Result:
     return min(results, key=lambda r: r.total_ms)
 
 
+def _read_cache() -> dict:
+    """The tuning cache, or an empty one when the file is missing or unreadable
+    (a write cut short by another process): the sweep then runs again."""
+    try:
+        return json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    except (OSError, ValueError):
+        return {}
+
+
 def cache_key(gpu_name: str, config) -> str:
     L = config.levels[0]
     fp = int(bool(getattr(config, "fingerprints", False)))
@@ -119,7 +128,7 @@ def tuned_shape(config, seed: int, keys, vals, qkeys, **grid) -> Shape:
     import torch
     name = torch.cuda.get_device_name()
     key = cache_key(name, config)
-    cache = json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    cache = _read_cache()
     if key in cache:
         return Shape(**cache[key]["shape"])
 
@@ -229,7 +238,7 @@ def tuned_batch_shape(make_configs, seeds, ins_ops, q_ops, nops, keys, vals, qke
     miss.  Returns (shape, results of the sweep or None when cached)."""
     import torch
     key = batch_cache_key(torch.cuda.get_device_name(), make_configs(16))
-    cache = json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    cache = _read_cache()
     if key in cache:
         return BatchShape(**cache[key]["shape"]), None
     res = sweep_batch(make_configs, seeds, ins_ops, q_ops, nops, keys, vals, qkeys, **grid)
