@@ -262,6 +262,11 @@ def test_server_large_requests_split_their_host_copies(pg):
         fq2 = np.zeros(n // 2, dtype=np.uint8)
         srv.poll(srv.submit(tid, pg.PG_OP_QUERY, keys[: n // 2], None, None, fq2), wait=True)
         assert not fq2[: n // 4].any() and fq2[n // 4:].all()
+        # the worker's time by stage covers the four requests' waves
+        tm = srv.timing()
+        waves, keys_run = srv.stats()
+        assert tm["waves"] == waves >= 4 and tm["requests"] == 4 and tm["keys"] == keys_run == 2 * n + n // 4 + n // 2
+        assert all(tm[k] >= 0 for k in tm if k.endswith("_s")) and tm["copy_in_s"] > 0 and tm["copy_out_s"] > 0
         srv.drop_table(tid)
     finally:
         srv.close()
