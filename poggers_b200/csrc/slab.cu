@@ -100,20 +100,57 @@ __device__ __forceinline__ uint32_t class_of(const set_desc &D, uint64_t size)
     return c;
 }
 
+// One malloc per request.  The lanes of a warp that ask the same class claim
+// together (one snapshot and atomicAnd serve them all), so the block first
+// orders its 256 requests by class in shared memory: a warp then holds one or
+// two classes instead of most of them, and a claim serves up to 32 objects.
+// Results go back to each request's own place.
+#ifndef PG_SET_MALLOC_SORT
+#define PG_SET_MALLOC_SORT 1
+#endif
 __global__ void __launch_bounds__(256) k_set_malloc(set_desc D, uint64_t n, const uint32_t *sizes, void **out,
                                                     unsigned long long *fails)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * blockDim.x;
+    const uint64_t i = base + threadIdx.x;
+#if PG_SET_MALLOC_SORT
+    // classes 0 .. D.n - 1, D.n = too large for every class, D.n + 1 = no request
+    __shared__ uint32_t cnt[PG_SLAB_MAX_CLASSES + 2];
+    __shared__ uint8_t cls[256];
+    __shared__ uint8_t from[256];
+    if (threadIdx.x < PG_SLAB_MAX_CLASSES + 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t c0 = i < n ? class_of(D, sizes[i]) : D.n + 1;
+    const uint32_t rank = atomicAdd(&cnt[c0], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t at = 0;
+        for (uint32_t c = 0; c < D.n + 2; c++) {
+            const uint32_t k = cnt[c];
+            cnt[c] = at;
+            at += k;
+        }
+    }
+    __syncthreads();
+    cls[cnt[c0] + rank] = (uint8_t)c0;
+    from[cnt[c0] + rank] = (uint8_t)threadIdx.x;
+    __syncthreads();
+    const uint32_t c = cls[threadIdx.x];
+    const uint64_t dst = base + from[threadIdx.x];
+    const unsigned peers = __match_any_sync(0xffffffffu, c);  // the lanes asking the same class claim together
+    if (c > D.n) return;  // no request here (the block's tail)
+#else
     if (i >= n) return;
     const uint32_t c = class_of(D, sizes[i]);
-    const unsigned am = __activemask();
-    const unsigned peers = __match_any_sync(am, c);  // the lanes asking the same class claim together
+    const uint64_t dst = i;
+    const unsigned peers = __match_any_sync(__activemask(), c);  // the lanes asking the same class claim together
+#endif
     void *p = nullptr;
     if (c < D.n) {
         const uint64_t off = slab_claim(D.s[c], peers);
         if (off != ~0ULL) p = D.s[c].pool + off * D.s[c].size;
     }
-    out[i] = p;
+    out[dst] = p;
     if (!p && fails) atomicAdd(fails, 1ULL);
 }
 
