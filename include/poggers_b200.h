@@ -522,13 +522,17 @@ pg_status pg_pslab_bulk_free(pg_pslab *a, void *const *d_ptrs, uint64_t n, uint6
  * per SM; *accesses_done receives the exact count (rounded up to whole
  * per-thread batches).  READ32: one 32-byte sector; READ64: two adjacent
  * sectors; READ32_CAS: one sector, then a CAS on its first 4-byte word with
- * the value read; RED32: an atomic add (no return) on a random 4-byte word.
+ * the value read; RED32: an atomic add (no return) on a random 4-byte word;
+ * READ32_CAS_NEXT: within a random 64-byte span, READ32_CAS on its first
+ * sector and a 2-byte store into its second (a split filter bucket's insert:
+ * claim a tag, then write its value).
  * CAS and RED modes modify d_buf.  d_sink (8 bytes) only keeps the loads.
  * --------------------------------------------------------------------------- */
 #define PG_DIAG_READ32 0
 #define PG_DIAG_READ64 1
 #define PG_DIAG_READ32_CAS 2
 #define PG_DIAG_RED32 3
+#define PG_DIAG_READ32_CAS_NEXT 4
 pg_status pg_diag_random_access(void *d_buf, uint64_t bytes, uint32_t mode, uint64_t accesses, uint64_t seed,
                                 uint32_t blocks_per_sm, uint64_t *accesses_done, uint64_t *d_sink,
                                 pg_stream_t stream);

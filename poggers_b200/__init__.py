@@ -33,7 +33,7 @@ LIB_PATH = Path(os.environ.get("POGGERS_B200_LIB", str(_PKG / "libpoggers_b200.s
 PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_NOMEM, PG_ERR_UNSUPPORTED, PG_ERR_FULL, PG_ERR_TIMEOUT, PG_ERR_TOO_LARGE = range(8)
 PG_STATIC_MAX_TABLES = 256
 PG_STATIC_MAX_OPS = 8192
-PG_DIAG_READ32, PG_DIAG_READ64, PG_DIAG_READ32_CAS, PG_DIAG_RED32 = 0, 1, 2, 3
+PG_DIAG_READ32, PG_DIAG_READ64, PG_DIAG_READ32_CAS, PG_DIAG_RED32, PG_DIAG_READ32_CAS_NEXT = 0, 1, 2, 3, 4
 PG_TABLE_SPLIT_BUCKETS = 1
 PG_TABLE_FINGERPRINTS = 2
 FMT_KV64, FMT_TAGVAL16, FMT_TAG16, FMT_PACKED_TAGVAL16, FMT_PACKED_TAGVAL8 = 0, 1, 2, 3, 4

@@ -795,7 +795,9 @@ def config_random(args):
     """The GPU's random-access ceilings, the filters' regime, measured by this
     library's own kernel (pg_diag_random_access): random 32-byte sectors, random
     64-byte pairs of sectors, a sector read followed by a CAS on it (an insert's
-    claim), and atomic adds with no return (write-only read-modify-writes), at
+    claim), the same plus a 2-byte store into the next sector (a split filter
+    bucket's insert: tag claimed, then its value written), and atomic adds with
+    no return (write-only read-modify-writes), at
     the filters' table sizes (512 MiB = the tags of a 2^28-slot TCF, 1 GiB =
     its tags and values, 8 GiB = a 2^32-slot tag-only filter).  Several
     accesses are in flight per thread; CUDA-event timed, best of 5 after a
@@ -804,7 +806,7 @@ def config_random(args):
     uint64 table's fingerprint words live there)."""
     import torch
     modes = {"read32": pg.PG_DIAG_READ32, "read64": pg.PG_DIAG_READ64, "read32_cas": pg.PG_DIAG_READ32_CAS,
-             "red32": pg.PG_DIAG_RED32}
+             "red32": pg.PG_DIAG_RED32, "read32_cas_next": pg.PG_DIAG_READ32_CAS_NEXT}
     if args.calibrate:
         # one launch per kind over a 1 GiB and a 32 MiB buffer (for an ncu capture of DRAM and L2 traffic)
         done = {}
@@ -816,7 +818,7 @@ def config_random(args):
                 torch.cuda.synchronize()
             del buf
         return {"config": "random", "calibrate": done}
-    sectors = {"read32": 1, "read64": 2, "read32_cas": 1, "red32": 1}
+    sectors = {"read32": 1, "read64": 2, "read32_cas": 1, "red32": 1, "read32_cas_next": 1}
     out = {"config": "random", "note": "G accesses/s; sector_g_per_s counts the 32-byte sectors read per access"}
     sink = torch.zeros(1, dtype=torch.int64, device="cuda")
     for log2_bytes in (25, 29, 30, 33):  # 32 MiB stays in L2: the L2's own rates

@@ -33,14 +33,16 @@ __device__ __forceinline__ void ld_sector(const unsigned char *p, unsigned long 
                  : "l"(p));
 }
 
-// MODE: PG_DIAG_READ32, PG_DIAG_READ64, PG_DIAG_READ32_CAS, PG_DIAG_RED32.
-// Unit = the aligned span one access picks at random: 32 B, 64 B, 32 B, 4 B.
+// MODE: PG_DIAG_READ32, PG_DIAG_READ64, PG_DIAG_READ32_CAS, PG_DIAG_RED32,
+// PG_DIAG_READ32_CAS_NEXT.  Unit = the aligned span one access picks at
+// random: 32 B, 64 B, 32 B, 4 B, 64 B.
 // Every offset is mulhi(hash, units) * unit < units * unit <= the buffer's bytes.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_random_access(unsigned char *buf, uint64_t units, uint64_t per_thread,
                                                        uint64_t seed, unsigned long long *sink)
 {
-    constexpr uint64_t kUnit = MODE == PG_DIAG_READ64 ? 64 : (MODE == PG_DIAG_RED32 ? 4 : 32);
+    constexpr uint64_t kUnit =
+        (MODE == PG_DIAG_READ64 || MODE == PG_DIAG_READ32_CAS_NEXT) ? 64 : (MODE == PG_DIAG_RED32 ? 4 : 32);
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long acc = 0;
     for (uint64_t j = 0; j < per_thread; j += kUnroll) {
@@ -61,13 +63,19 @@ __global__ void __launch_bounds__(256) k_random_access(unsigned char *buf, uint6
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) acc ^= w[u][0] ^ w[u][3];
             }
-            if constexpr (MODE == PG_DIAG_READ32_CAS) {
+            if constexpr (MODE == PG_DIAG_READ32_CAS || MODE == PG_DIAG_READ32_CAS_NEXT) {
                 // claim the sector's first word: a CAS on the value just read
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
                     const unsigned seen = (unsigned)v[u][0];
                     acc ^= atomicCAS(reinterpret_cast<unsigned *>(buf + off[u]), seen, seen + 1u);
                 }
+            }
+            if constexpr (MODE == PG_DIAG_READ32_CAS_NEXT) {
+                // then the value: 2 bytes of the span's second sector
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u)
+                    *reinterpret_cast<unsigned short *>(buf + off[u] + 32 + 2 * (u & 15)) = (unsigned short)v[u][1];
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) acc ^= v[u][0] ^ v[u][1] ^ v[u][2] ^ v[u][3];
@@ -84,7 +92,8 @@ pg_status pg_diag_random_access(void *d_buf, uint64_t bytes, uint32_t mode, uint
                                 uint32_t blocks_per_sm, uint64_t *accesses_done, uint64_t *d_sink,
                                 pg_stream_t stream)
 {
-    if (!d_buf || !d_sink || mode > PG_DIAG_RED32 || bytes < 64 || ((uintptr_t)d_buf & 63)) return PG_ERR_INVALID;
+    if (!d_buf || !d_sink || mode > PG_DIAG_READ32_CAS_NEXT || bytes < 64 || ((uintptr_t)d_buf & 63))
+        return PG_ERR_INVALID;
     if (blocks_per_sm == 0) blocks_per_sm = 8;
     if (blocks_per_sm > 8) return PG_ERR_INVALID;  // 8 x 256 threads fill an SM
     int dev = 0, sms = 0;
@@ -93,7 +102,8 @@ pg_status pg_diag_random_access(void *d_buf, uint64_t bytes, uint32_t mode, uint
         cudaGetLastError();
         return PG_ERR_CUDA;
     }
-    const uint64_t unit = mode == PG_DIAG_READ64 ? 64 : (mode == PG_DIAG_RED32 ? 4 : 32);
+    const uint64_t unit =
+        (mode == PG_DIAG_READ64 || mode == PG_DIAG_READ32_CAS_NEXT) ? 64 : (mode == PG_DIAG_RED32 ? 4 : 32);
     const uint64_t units = bytes / unit;
     const uint64_t threads = (uint64_t)sms * blocks_per_sm * 256;
     uint64_t per_thread = (accesses + threads - 1) / threads;
@@ -109,6 +119,9 @@ pg_status pg_diag_random_access(void *d_buf, uint64_t bytes, uint32_t mode, uint
     case PG_DIAG_READ64: k_random_access<PG_DIAG_READ64><<<grid, block, 0, s>>>(b, units, per_thread, seed, sk); break;
     case PG_DIAG_READ32_CAS:
         k_random_access<PG_DIAG_READ32_CAS><<<grid, block, 0, s>>>(b, units, per_thread, seed, sk);
+        break;
+    case PG_DIAG_READ32_CAS_NEXT:
+        k_random_access<PG_DIAG_READ32_CAS_NEXT><<<grid, block, 0, s>>>(b, units, per_thread, seed, sk);
         break;
     default: k_random_access<PG_DIAG_RED32><<<grid, block, 0, s>>>(b, units, per_thread, seed, sk); break;
     }
