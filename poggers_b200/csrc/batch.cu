@@ -49,7 +49,10 @@ __global__ void __launch_bounds__(1024) k_batch_plan(batch_args a)
     for (uint32_t base = 0; base < nops; base += blockDim.x) {
         const uint32_t j = base + threadIdx.x;
         unsigned long long v = 0;
-        if (j < nops) v = (a.ops[j].count + kBatchChunk - 1) / kBatchChunk;
+        if (j < nops) {
+            const uint64_t ck = batch_chunk_keys(a, a.ops[j]);
+            v = (a.ops[j].count + ck - 1) / ck;
+        }
         // inclusive scan in the warp, then across warps
         unsigned long long x = v;
         for (int o = 1; o < 32; o <<= 1) {

@@ -41,9 +41,10 @@ __global__ void __launch_bounds__(256) k_batch_packed(batch_args a)
                         : od.op == PG_OP_REMOVE    ? (int)POP_REMOVE
                                                    : (int)POP_INSERT_DELETE;
         const bool counts_hits = opk == POP_QUERY || opk == POP_REMOVE;
-        const uint64_t first = od.offset + (c - a.chunk_start[lo]) * kBatchChunk;
+        const uint64_t ck = batch_chunk_keys(a, od);
+        const uint64_t first = od.offset + (c - a.chunk_start[lo]) * ck;
         const uint64_t end = od.offset + od.count;
-        const uint64_t stop = first + kBatchChunk < end ? first + kBatchChunk : end;
+        const uint64_t stop = first + ck < end ? first + ck : end;
         uint32_t cnt = 0;
         for (uint64_t i = first + gi; i < stop; i += kGroupsPerWarp) {
             const uint64_t key = __ldg(a.keys + i);
