@@ -51,6 +51,7 @@ struct batch_args {
 #ifndef PG_BATCH_INSERT_BUCKETS
 #define PG_BATCH_INSERT_BUCKETS 128
 #endif
+constexpr uint64_t kBatchMaxChunk = 16384;
 __device__ __forceinline__ uint64_t batch_chunk_keys(const batch_args &a, const pg_op_desc &od)
 {
     if (PG_BATCH_INSERT_BUCKETS == 0 || (od.op != PG_OP_INSERT && od.op != PG_OP_INSERT_WITH_DELETE) ||
@@ -59,7 +60,9 @@ __device__ __forceinline__ uint64_t batch_chunk_keys(const batch_args &a, const 
     const uint64_t nb = a.tables[od.table].lv[0].nbmod.d;
     const uint64_t chunks = nb >= PG_BATCH_INSERT_BUCKETS ? nb / PG_BATCH_INSERT_BUCKETS : 1;
     const uint64_t per = (od.count + chunks - 1) / chunks;
-    return per > kBatchChunk ? per : kBatchChunk;
+    // a request far larger than its table (mostly failing inserts) still
+    // spreads over warps: at most kBatchMaxChunk keys per chunk
+    return per > kBatchChunk ? (per < kBatchMaxChunk ? per : kBatchMaxChunk) : kBatchChunk;
 }
 
 // one block: exclusive scan of ceil(count / batch_chunk_keys) over the requests
